@@ -1,0 +1,85 @@
+// fvm_internal.cuh -- device data layout and kernel launch interface shared
+// by the library's translation units.  Not part of the public C ABI.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include "fvm_math.cuh"
+
+namespace fvm {
+
+// A solve's grid.  Fields are SoA float planes of ny rows x `pitch` floats
+// (pitch = nx rounded up to 32, so every row starts 128-byte aligned); the 5
+// conserved planes of one state (rho, rho_u, rho_v, E, rho_e) are contiguous,
+// plane k at base + k*plane.
+struct GridDesc {
+    int nx, ny;
+    int pitch;
+    long long plane;
+    float dx, dy;
+};
+
+// Static per-ghost-cell data, built once per geometry: pitched cell index,
+// unit SDF normal, and the candidate fluid neighbours in the order the
+// reference's best-neighbour search would prefer them (descending dot with
+// the normal, ties to the earlier neighbour; src/solver.cu:2068-2098).
+// Candidate nibble k: bits 0-2 neighbour code in the reference order
+// {(-1,0),(1,0),(0,-1),(0,1),(-1,-1),(1,-1),(-1,1),(1,1)}, bit 3 set when the
+// neighbour is itself a ghost cell.
+struct GhostInfo {
+    int pidx;
+    int i, j;
+    float gx, gy;
+    uint32_t cand;
+    int count;
+};
+
+// Device-resident scalars of one solve.
+struct DevScalars {
+    float red[2];     // running maxima of the fused CFL reduction (speed, nu)
+    float cfl[2];     // maxima of the last completed step
+    float dt;         // dt the next step uses (read by the step kernels)
+    float t;          // simulated time (advanced on the device under recompute)
+    unsigned counter; // last-block counter of the ghost pass
+    unsigned err;     // error word (kErrTimeout, kErrNonFinite)
+    unsigned nonfinite;
+    float dt_last;    // dt of the last completed step (recompute policy)
+    double diag[16];  // FP64 diagnostic accumulators
+};
+
+// Step-kernel arguments common to all stage kernels.
+struct StepArgs {
+    GridDesc g;
+    float *out;            // output state (5 planes)
+    const uint8_t *mask;   // pitched mask bytes (pitch bytes per row)
+    DevScalars *sc;        // dt / reductions / error word
+    Freestream fs;
+    WallParams wall;
+    float prandtl;
+    int ref_prandtl;
+    int rows_per_cta;
+    int apply_bc;          // phase-1 boundary conditions on the output
+    int cfl;               // 0: none, 1: wave speed, 2: wave speed + kinematic viscosity
+    float dt_scale;        // stage dt = sc->dt * dt_scale (0.5 for the viscous half steps)
+};
+
+struct GhostArgs {
+    GridDesc g;
+    const GhostInfo *list;
+    int n;
+    float *A;              // phase-1 state: non-ghost neighbours read here, ghost cells written here
+    const float *B1;       // pre-BC ghost values: B2 ? 0.5*B1 + 0.5*B2 : B1
+    const float *B2;
+    DevScalars *sc;
+    Freestream fs;
+    WallParams wall;
+    int cfl;               // 0: none, 1: speed, 2: speed + nu (T from the pre-BC ghost state)
+    int finalize;          // last block publishes the step's CFL maxima and next dt
+    int recompute_dt;
+    float cfl_num, cfl_visc, min_dx;
+    int viscous;
+};
+
+}  // namespace fvm

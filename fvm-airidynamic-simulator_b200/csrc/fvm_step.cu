@@ -1,0 +1,706 @@
+// fvm_step.cu -- the per-step hot path: fused marching RK-stage kernels, the
+// viscous half step, the ghost-cell pass and the CFL reduction.
+//
+// Structure of a marching kernel.  A CTA of NT threads owns a strip of
+// W = NT-4 output columns and `rows` output rows.  It walks the strip from
+// bottom to top one row at a time.  Each incoming row (the 5 conserved planes
+// of the input state, columns [i0-4, i0+W+4)) is staged into a shared-memory
+// ring by one 3-D TMA load (x, y, field) signalled on an mbarrier, issued
+// ring-3 rows ahead.  Per row:
+//   phase 1  primitives of the incoming row r on NT columns (one per thread)
+//   phase 2  x-faces of row r (W+1 faces) and y-faces between rows r-2, r-1
+//   phase 3  update of row r-2 from the faces, RK blend, phase-1 boundary
+//            conditions, CFL contribution, coalesced store
+// so every face flux is computed exactly once per strip and each input cell
+// crosses HBM once (halo re-reads hit L2).  Domain-edge halos use the
+// reference's clamp-to-edge semantics (src/solver.cu:1484-1488): rows by
+// clamping the TMA row coordinate, columns by clamping the shared-memory column.
+#include <cstdio>
+
+#include "fvm_kernels.cuh"
+#include "fvm_tma.cuh"
+
+namespace fvm {
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return max(lo, min(v, hi)); }
+
+__device__ __forceinline__ void record_error(DevScalars *sc, unsigned bit) { atomicOr(&sc->err, bit); }
+
+// Block-wide max of two non-negative values, one atomic per CTA.
+template <int NT>
+__device__ __forceinline__ void block_max2_publish(float a, float b, float *dst) {
+    __shared__ float ws[2][NT / 32];
+    a = warp_max(a);
+    b = warp_max(b);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) {
+        ws[0][w] = a;
+        ws[1][w] = b;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float ma = 0.0f, mb = 0.0f;
+        for (int k = 0; k < NT / 32; k++) {
+            ma = fmaxf(ma, ws[0][k]);
+            mb = fmaxf(mb, ws[1][k]);
+        }
+        atomic_max_nonneg(&dst[0], ma);
+        atomic_max_nonneg(&dst[1], mb);
+    }
+}
+
+// Width of one TMA box of the halo'd input (a TMA box spans at most 256
+// elements per dimension; 132 floats = 528 B keeps every box start 16-byte
+// aligned).  A staged row is NB boxes, each stored as [field][kBox].
+constexpr int kBox = 132;
+
+// Address of (field f, staged column x) in a ring slot of NB boxes.
+template <int NB>
+__device__ __forceinline__ float ring_at(const float *slot_base, int f, int x) {
+    if (NB == 1) return slot_base[f * kBox + x];
+    const int b = x / kBox;
+    return slot_base[(b * 5 + f) * kBox + (x - b * kBox)];
+}
+
+template <int NT, int K, int STAGE>
+struct StageLayout {
+    static constexpr int W = NT - 4;   // output columns
+    static constexpr int NB = (NT + 4 + kBox - 1) / kBox;  // TMA boxes per row
+    static constexpr int BW = NB * kBox;  // staged columns [i0-4, i0-4+BW)
+    static constexpr int PR = 5;       // primitive / mask ring (rows)
+    static constexpr int XR = 3;       // x-face ring
+    static constexpr int YR = 2;       // y-face ring
+    static constexpr size_t raw_off = 0;
+    static constexpr size_t raw_bytes = (size_t)K * 5 * BW * 4;
+    static constexpr size_t bl_off = raw_off + raw_bytes;
+    static constexpr size_t bl_bytes = STAGE == 2 ? (size_t)K * 5 * W * 4 : 0;
+    static constexpr size_t p_off = bl_off + bl_bytes;
+    static constexpr size_t p_bytes = (size_t)PR * NT * 16;
+    static constexpr size_t x_off = p_off + p_bytes;
+    static constexpr size_t x_bytes = (size_t)XR * 5 * NT * 4;
+    static constexpr size_t y_off = x_off + x_bytes;
+    static constexpr size_t y_bytes = (size_t)YR * 5 * NT * 4;
+    static constexpr size_t m_off = y_off + y_bytes;
+    static constexpr size_t m_bytes = (size_t)PR * NT;
+    static constexpr size_t bar_off = (m_off + m_bytes + 15) & ~(size_t)15;
+    static constexpr size_t total = bar_off + K * 8;
+    static constexpr uint32_t tx_bytes = 5 * BW * 4 + (STAGE == 2 ? 5 * W * 4 : 0);
+};
+
+// Inviscid SSP-RK2 stage (computeFluxesKernel + updateKernel + [blend] +
+// phase-1 BC, src/solver.cu:1450-1876, :949-967, :1891-2042).
+template <int NT, int K, int STAGE, int SCHEME, int LIM>
+__global__ void __launch_bounds__(NT) k_stage(const __grid_constant__ CUtensorMap tm_in,
+                                              const __grid_constant__ CUtensorMap tm_blend, const StepArgs a) {
+    using L = StageLayout<NT, K, STAGE>;
+    constexpr int W = L::W, BW = L::BW, PR = L::PR, XR = L::XR;
+    static_assert(L::total <= 227 * 1024, "shared memory");
+    constexpr int AHEAD = K - 3;
+    extern __shared__ __align__(128) unsigned char smem[];
+    float *raw = reinterpret_cast<float *>(smem + L::raw_off);
+    float *bl = reinterpret_cast<float *>(smem + L::bl_off);
+    float4 *P = reinterpret_cast<float4 *>(smem + L::p_off);
+    float *X = reinterpret_cast<float *>(smem + L::x_off);
+    float *Y = reinterpret_cast<float *>(smem + L::y_off);
+    uint8_t *M = smem + L::m_off;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bar_off);
+
+    const GridDesc g = a.g;
+    const int nx = g.nx, ny = g.ny;
+    const int t = threadIdx.x;
+    const int i0 = blockIdx.x * W;
+    const int j0 = blockIdx.y * a.rows_per_cta;
+    const int j1 = min(j0 + a.rows_per_cta, ny);
+    const int rs = j0 - 2;
+    const int nrows = (j1 + 1) - rs + 1;  // incoming rows rs .. j1+1
+
+    const float dt = a.sc->dt * a.dt_scale;
+    const UpdateArgs ua{dt, 1.0f / g.dx, 1.0f / g.dy};
+
+    if (t == 0) {
+        prefetch_tensormap(&tm_in);
+        if (STAGE == 2) prefetch_tensormap(&tm_blend);
+        for (int k = 0; k < K; k++) mbar_init(&bars[k], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    auto issue = [&](int q) {
+        const int slot = q % K;
+        const int row = clampi(rs + q, 0, ny - 1);
+        mbar_arrive_expect_tx(&bars[slot], L::tx_bytes);
+#pragma unroll
+        for (int b = 0; b < L::NB; b++)
+            tma_load_3d(raw + (size_t)slot * 5 * BW + b * 5 * kBox, &tm_in, &bars[slot], i0 - 4 + b * kBox, row, 0);
+        if (STAGE == 2) tma_load_3d(bl + (size_t)slot * 5 * W, &tm_blend, &bars[slot], i0, row, 0);
+    };
+    if (t == 0)
+        for (int q = 0; q < min(AHEAD, nrows); q++) issue(q);
+
+    float lmax_speed = 0.0f;
+    int issued = min(AHEAD, nrows);
+    bool aborted = false;
+
+    for (int q = 0; q < nrows; q++) {
+        const int r = rs + q;
+        const int slot = q % K;
+        // ---- phase 1: primitives + mask of the incoming row
+        bool ok = mbar_wait_bounded(&bars[slot], (uint32_t)((q / K) & 1));
+        if (ok) {
+            const int i = i0 - 2 + t;
+            const int ic = clampi(i, 0, nx - 1);
+            const int rc = ic - i0 + 4;
+            const float *src = raw + (size_t)slot * 5 * BW;
+            float u, v, p, T;
+            const float rho = ring_at<L::NB>(src, 0, rc);
+            prim_from_cons(rho, ring_at<L::NB>(src, 1, rc), ring_at<L::NB>(src, 2, rc), ring_at<L::NB>(src, 3, rc),
+                           ring_at<L::NB>(src, 4, rc), u, v, p, T);
+            P[(r % PR + PR) % PR * NT + t] = make_float4(rho, u, v, p);
+            M[(r % PR + PR) % PR * NT + t] = a.mask[(size_t)clampi(r, 0, ny - 1) * g.pitch + ic];
+        }
+        if (__syncthreads_or(!ok)) {
+            aborted = true;
+            break;
+        }
+        const int sr = (r % PR + PR) % PR;
+        // ---- phase 2a: x-faces of row r (face of cell i0-1+t, t in [0, W])
+        if (r >= j0 && t <= W) {
+            const float4 *Pr = P + sr * NT;
+            const uint32_t mb = M[sr * NT + t + 1];
+            const float4 m1 = Pr[t], aa = Pr[t + 1], bb = Pr[t + 2], p2 = Pr[t + 3];
+            float f[5];
+            face_flux<true, SCHEME, LIM>((mb & MB_XV) != 0, (mb & MB_XN) != 0, Prim{m1.x, m1.y, m1.z, m1.w},
+                                         Prim{aa.x, aa.y, aa.z, aa.w}, Prim{bb.x, bb.y, bb.z, bb.w},
+                                         Prim{p2.x, p2.y, p2.z, p2.w}, f);
+            float *Xs = X + (size_t)((r % XR + XR) % XR) * 5 * NT;
+#pragma unroll
+            for (int k = 0; k < 5; k++) Xs[k * NT + t] = f[k];
+        }
+        // ---- phase 2b: y-face between rows r-2 and r-1 at column i0+t
+        if (r >= j0 + 1 && t < W) {
+            const int c = t + 2;
+            const float4 m1 = P[((r - 3) % PR + PR) % PR * NT + c];
+            const float4 aa = P[((r - 2) % PR + PR) % PR * NT + c];
+            const float4 bb = P[((r - 1) % PR + PR) % PR * NT + c];
+            const float4 p2 = P[sr * NT + c];
+            const uint32_t mb = M[((r - 2) % PR + PR) % PR * NT + c];
+            float f[5];
+            face_flux<false, SCHEME, LIM>((mb & MB_YV) != 0, (mb & MB_YN) != 0, Prim{m1.x, m1.y, m1.z, m1.w},
+                                          Prim{aa.x, aa.y, aa.z, aa.w}, Prim{bb.x, bb.y, bb.z, bb.w},
+                                          Prim{p2.x, p2.y, p2.z, p2.w}, f);
+            float *Ys = Y + (size_t)((r - 2) & 1) * 5 * NT;
+#pragma unroll
+            for (int k = 0; k < 5; k++) Ys[k * NT + t] = f[k];
+        }
+        fence_proxy_async_smem();
+        __syncthreads();
+        // refill the ring slot freed by row q-3 (last read in phase 3 of q-1)
+        if (t == 0 && issued < nrows && issued <= q + AHEAD) {
+            issue(issued);
+            ++issued;
+        }
+        // ---- phase 3: update row r-2
+        const int urow = r - 2;
+        const int i = i0 + t;
+        if (urow >= j0 && urow < j1 && t < W && i < nx) {
+            const int c = t + 2;
+            const int su = (urow % PR + PR) % PR;
+            const uint32_t mb = M[su * NT + c];
+            const int uslot = (q - 2) % K;
+            const float *src = raw + (size_t)uslot * 5 * BW;
+            float Uc[5], Un[5];
+#pragma unroll
+            for (int k = 0; k < 5; k++) Uc[k] = ring_at<L::NB>(src, k, t + 4);
+            if (mb & MB_WALL) {
+#pragma unroll
+                for (int k = 0; k < 5; k++) Un[k] = Uc[k];
+            } else {
+                const float *Xs = X + (size_t)((urow % XR + XR) % XR) * 5 * NT;
+                const float *Yt = Y + (size_t)(urow & 1) * 5 * NT;
+                const float *Yb = Y + (size_t)((urow - 1) & 1) * 5 * NT;
+                float fR[5], fL[5], fT[5], fB[5];
+#pragma unroll
+                for (int k = 0; k < 5; k++) {
+                    fR[k] = Xs[k * NT + t + 1];
+                    fL[k] = Xs[k * NT + t];
+                    fT[k] = Yt[k * NT + t];
+                    fB[k] = Yb[k * NT + t];
+                }
+                const float4 pc = P[su * NT + c];
+                const float rxR = P[su * NT + c + 1].x, rxL = P[su * NT + c - 1].x;
+                const float ryT = P[((urow + 1) % PR + PR) % PR * NT + c].x;
+                const float ryB = P[((urow - 1) % PR + PR) % PR * NT + c].x;
+                const bool edge_x = (i == 0 || i == nx - 1);
+                const bool edge_y = (urow == 0 || urow == ny - 1);
+                update_cell(Uc, fR, fL, fT, fB, rxR, rxL, ryT, ryB, pc.w, edge_x, edge_y, !edge_x && !edge_y, ua,
+                            Un);
+            }
+            if (STAGE == 2) {
+                const float *b = bl + (size_t)uslot * 5 * W;
+#pragma unroll
+                for (int k = 0; k < 5; k++) Un[k] = 0.5f * b[k * W + t] + 0.5f * Un[k];
+            }
+            const uint32_t ctype = mb_type(mb);
+            if (a.apply_bc) bc_pointwise(Un, ctype, i, urow, nx, ny, a.fs);
+            if (a.cfl && ctype != CT_GHOST) {
+                float uu, vv, pp, TT;
+                prim_from_cons(Un[0], Un[1], Un[2], Un[3], Un[4], uu, vv, pp, TT);
+                lmax_speed = fmaxf(lmax_speed, wave_speed(uu, vv, pp, Un[0]));
+            }
+            float *dst = a.out + (size_t)urow * g.pitch + i;
+#pragma unroll
+            for (int k = 0; k < 5; k++) dst[k * g.plane] = Un[k];
+        }
+    }
+    if (aborted) {
+        if (t == 0) {
+            record_error(a.sc, kErrTimeout);
+            // drain loads still in flight before the CTA's shared memory is released
+            for (int q = 0; q < issued; q++) mbar_wait_bounded(&bars[q % K], (uint32_t)((q / K) & 1), 20000000LL);
+        }
+        return;
+    }
+    if (a.cfl) block_max2_publish<NT>(lmax_speed, 0.0f, a.sc->red);
+}
+
+template <int NT, int K>
+struct ViscLayout {
+    static constexpr int W = NT - 4;
+    static constexpr int NB = (NT + 4 + kBox - 1) / kBox;
+    static constexpr int BW = NB * kBox;
+    static constexpr int PR = 5;
+    static constexpr int TR = 3;
+    static constexpr size_t raw_off = 0;
+    static constexpr size_t raw_bytes = (size_t)K * 5 * BW * 4;
+    static constexpr size_t p_off = raw_off + raw_bytes;
+    static constexpr size_t p_bytes = (size_t)PR * NT * 16;
+    static constexpr size_t t_off = p_off + p_bytes;
+    static constexpr size_t t_bytes = (size_t)TR * 5 * NT * 4;
+    static constexpr size_t m_off = t_off + t_bytes;
+    static constexpr size_t m_bytes = (size_t)PR * NT;
+    static constexpr size_t bar_off = (m_off + m_bytes + 15) & ~(size_t)15;
+    static constexpr size_t total = bar_off + K * 8;
+    static constexpr uint32_t tx_bytes = 5 * BW * 4;
+};
+
+// Viscous half step (fusedViscousDiffusionKernel, src/solver.cu:2251-2511),
+// out of place, marching like k_stage.  Primitives (u, v, T) of the input on
+// NT columns, stress/heat flux on NT-2 columns, update on W = NT-4 columns.
+template <int NT, int K>
+__global__ void __launch_bounds__(NT) k_viscous(const __grid_constant__ CUtensorMap tm_in, const StepArgs a) {
+    using L = ViscLayout<NT, K>;
+    constexpr int W = L::W, BW = L::BW, PR = L::PR, TR = L::TR;
+    constexpr int AHEAD = K - 3;
+    extern __shared__ __align__(128) unsigned char smem[];
+    float *raw = reinterpret_cast<float *>(smem + L::raw_off);
+    float4 *P = reinterpret_cast<float4 *>(smem + L::p_off);  // {u, v, T, -}
+    float *Tq = reinterpret_cast<float *>(smem + L::t_off);   // {txx, tyy, txy, qx, qy}
+    uint8_t *M = smem + L::m_off;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bar_off);
+
+    const GridDesc g = a.g;
+    const int nx = g.nx, ny = g.ny;
+    const int t = threadIdx.x;
+    const int i0 = blockIdx.x * W;
+    const int j0 = blockIdx.y * a.rows_per_cta;
+    const int j1 = min(j0 + a.rows_per_cta, ny);
+    const int rs = j0 - 2;
+    const int nrows = (j1 + 1) - rs + 1;
+
+    const float dt = a.sc->dt * a.dt_scale;
+    ViscArgs va;
+    va.inv_2dx = 0.5f / g.dx;
+    va.inv_2dy = 0.5f / g.dy;
+    va.inv_dx = 1.0f / g.dx;
+    va.inv_dy = 1.0f / g.dy;
+    va.prandtl = a.prandtl;
+    va.ref_prandtl = a.ref_prandtl != 0;
+
+    if (t == 0) {
+        prefetch_tensormap(&tm_in);
+        for (int k = 0; k < K; k++) mbar_init(&bars[k], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    auto issue = [&](int q) {
+        const int slot = q % K;
+        const int row = clampi(rs + q, 0, ny - 1);
+        mbar_arrive_expect_tx(&bars[slot], L::tx_bytes);
+#pragma unroll
+        for (int b = 0; b < L::NB; b++)
+            tma_load_3d(raw + (size_t)slot * 5 * BW + b * 5 * kBox, &tm_in, &bars[slot], i0 - 4 + b * kBox, row, 0);
+    };
+    if (t == 0)
+        for (int q = 0; q < min(AHEAD, nrows); q++) issue(q);
+    int issued = min(AHEAD, nrows);
+    bool aborted = false;
+    float lmax_speed = 0.0f, lmax_nu = 0.0f;
+
+    for (int q = 0; q < nrows; q++) {
+        const int r = rs + q;
+        const int slot = q % K;
+        const int sr = (r % PR + PR) % PR;
+        bool ok = mbar_wait_bounded(&bars[slot], (uint32_t)((q / K) & 1));
+        if (ok) {
+            const int i = i0 - 2 + t;
+            const int ic = clampi(i, 0, nx - 1);
+            const int rc = ic - i0 + 4;
+            const float *src = raw + (size_t)slot * 5 * BW;
+            float u, v, p, T;
+            prim_from_cons(ring_at<L::NB>(src, 0, rc), ring_at<L::NB>(src, 1, rc), ring_at<L::NB>(src, 2, rc),
+                           ring_at<L::NB>(src, 3, rc), ring_at<L::NB>(src, 4, rc), u, v, p, T);
+            P[sr * NT + t] = make_float4(u, v, T, 0.0f);
+            M[sr * NT + t] = a.mask[(size_t)clampi(r, 0, ny - 1) * g.pitch + ic];
+        }
+        if (__syncthreads_or(!ok)) {
+            aborted = true;
+            break;
+        }
+        // ---- phase 2: stress and heat flux of row r-1 at column i0-1+t
+        const int trow = r - 1;
+        if (trow >= j0 - 1 && t < NT - 2) {
+            const int i = i0 - 1 + t;
+            const int c = t + 1;
+            const int s0 = ((trow) % PR + PR) % PR, sN = sr, sS = ((trow - 1) % PR + PR) % PR;
+            float out[5];
+            const uint32_t ct = mb_type(M[s0 * NT + c]);
+            if (i < 0 || i >= nx || trow < 0 || trow >= ny || ct == CT_SOLID) {
+#pragma unroll
+                for (int k = 0; k < 5; k++) out[k] = 0.0f;
+            } else {
+                const float4 C = P[s0 * NT + c], E = P[s0 * NT + c + 1], Wc = P[s0 * NT + c - 1];
+                const float4 N = P[sN * NT + c], S = P[sS * NT + c];
+                stress_heat(C.x, C.y, C.z, E.x, Wc.x, N.x, S.x, E.y, Wc.y, N.y, S.y, E.z, Wc.z, N.z, S.z, i == 0,
+                            i == nx - 1, trow == 0, trow == ny - 1, va, out);
+            }
+            float *Ts = Tq + (size_t)((trow % TR + TR) % TR) * 5 * NT;
+#pragma unroll
+            for (int k = 0; k < 5; k++) Ts[k * NT + t] = out[k];
+        }
+        fence_proxy_async_smem();
+        __syncthreads();
+        if (t == 0 && issued < nrows && issued <= q + AHEAD) {
+            issue(issued);
+            ++issued;
+        }
+        // ---- phase 3: viscous update of row r-2 at column i0+t
+        const int urow = r - 2;
+        const int i = i0 + t;
+        if (urow >= j0 && urow < j1 && t < W && i < nx) {
+            const int c = t + 2;  // primitive column
+            const int tc = t + 1; // stress column
+            const int su = (urow % PR + PR) % PR;
+            const uint32_t mb = M[su * NT + c];
+            const uint32_t ctype = mb_type(mb);
+            const int uslot = (q - 2) % K;
+            const float *src = raw + (size_t)uslot * 5 * BW;
+            float U[5];
+#pragma unroll
+            for (int k = 0; k < 5; k++) U[k] = ring_at<L::NB>(src, k, t + 4);
+            const float4 pc = P[su * NT + c];
+            if (ctype == CT_FLUID && i > 0 && i < nx - 1 && urow > 0 && urow < ny - 1) {
+                const float *T0 = Tq + (size_t)((urow % TR + TR) % TR) * 5 * NT;
+                const float *TN = Tq + (size_t)(((urow + 1) % TR + TR) % TR) * 5 * NT;
+                const float *TS = Tq + (size_t)(((urow - 1) % TR + TR) % TR) * 5 * NT;
+                float tC[5], tE[5], tW[5], tNn[5], tSs[5];
+#pragma unroll
+                for (int k = 0; k < 5; k++) {
+                    tC[k] = T0[k * NT + tc];
+                    tE[k] = T0[k * NT + tc + 1];
+                    tW[k] = T0[k * NT + tc - 1];
+                    tNn[k] = TN[k * NT + tc];
+                    tSs[k] = TS[k * NT + tc];
+                }
+                const float4 E = P[su * NT + c + 1], Wc = P[su * NT + c - 1];
+                const float4 N = P[((urow + 1) % PR + PR) % PR * NT + c];
+                const float4 S = P[((urow - 1) % PR + PR) % PR * NT + c];
+                float rhs[4];
+                viscous_rhs(tC, tE, tW, tNn, tSs, E.x, Wc.x, N.x, S.x, E.y, Wc.y, N.y, S.y, va, rhs);
+                U[1] += dt * rhs[0];
+                U[2] += dt * rhs[1];
+                U[3] += dt * rhs[2];
+                U[4] += dt * rhs[3];
+            }
+            if (a.apply_bc) bc_pointwise(U, ctype, i, urow, nx, ny, a.fs);
+            if (a.cfl && ctype != CT_GHOST) {
+                float uu, vv, pp, TT;
+                prim_from_cons(U[0], U[1], U[2], U[3], U[4], uu, vv, pp, TT);
+                lmax_speed = fmaxf(lmax_speed, wave_speed(uu, vv, pp, U[0]));
+                if (a.cfl == 2) {
+                    const float mu = (ctype == CT_SOLID) ? 0.0f : sutherland_mu(pc.z);
+                    lmax_nu = fmaxf(lmax_nu, mu / (U[0] + 1e-10f));
+                }
+            }
+            float *dst = a.out + (size_t)urow * g.pitch + i;
+#pragma unroll
+            for (int k = 0; k < 5; k++) dst[k * g.plane] = U[k];
+        }
+    }
+    if (aborted) {
+        if (t == 0) {
+            record_error(a.sc, kErrTimeout);
+            for (int q = 0; q < issued; q++) mbar_wait_bounded(&bars[q % K], (uint32_t)((q / K) & 1), 20000000LL);
+        }
+        return;
+    }
+    if (a.cfl) block_max2_publish<NT>(lmax_speed, lmax_nu, a.sc->red);
+}
+
+// ------------------------------------------------------------- ghost pass
+__constant__ int c_nbr[8][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}, {-1, -1}, {1, -1}, {-1, 1}, {1, 1}};
+
+__device__ __forceinline__ float pre_bc(const GhostArgs &a, long long q, int k) {
+    const long long o = (long long)k * a.g.plane + q;
+    return a.B2 ? (0.5f * a.B1[o] + 0.5f * a.B2[o]) : a.B1[o];
+}
+
+// Publishes the completed step's CFL maxima and, under the recompute policy,
+// the next step's dt (readTimeStepResult, src/solver.cu:3250-3265, in IEEE
+// float like the reference's host code) and the advanced simulated time.
+__device__ void finalize_cfl(const GhostArgs &a) {
+    DevScalars *sc = a.sc;
+    volatile float *red = sc->red;
+    float ms = red[0], mn = red[1];
+    sc->cfl[0] = ms;
+    sc->cfl[1] = mn;
+    if (a.recompute_dt) {
+        float used = sc->dt;
+        sc->dt_last = used;
+        sc->t = __fadd_rn(sc->t, used);
+        float d = __fdiv_rn(__fmul_rn(a.cfl_num, a.min_dx), __fadd_rn(ms, 1e-10f));
+        if (a.viscous) {
+            float dv = __fdiv_rn(__fmul_rn(__fmul_rn(a.cfl_visc, a.min_dx), a.min_dx), __fadd_rn(mn, 1e-10f));
+            d = fminf(d, dv);
+        }
+        sc->dt = d;
+    }
+    red[0] = 0.0f;
+    red[1] = 0.0f;
+    __threadfence();
+    sc->counter = 0;
+}
+
+// Ghost cells (src/solver.cu:2045-2225) with phase-2 semantics: neighbours
+// are read from the phase-1 state A, except neighbours that are themselves
+// ghost cells, whose pre-call value comes from B1/B2.
+__global__ void __launch_bounds__(128) k_ghost(const GhostArgs a) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    float ls = 0.0f, ln = 0.0f;
+    if (k < a.n) {
+        const GhostInfo gi = a.list[k];
+        const long long plane = a.g.plane;
+        long long best = -1;
+        bool best_gh = false;
+        for (int m = 0; m < gi.count; m++) {
+            const int code = (gi.cand >> (4 * m)) & 0xF;
+            const int d = code & 7;
+            const bool gh = (code & 8) != 0;
+            const long long q = (long long)gi.pidx + c_nbr[d][0] + (long long)c_nbr[d][1] * a.g.pitch;
+            const float rq = gh ? pre_bc(a, q, 0) : a.A[q];
+            if (rq >= MIN_DENSITY) {
+                best = q;
+                best_gh = gh;
+                break;
+            }
+        }
+        float out[5];
+        if (best < 0) {
+            const float e_inf = a.fs.p / (GAMMA - 1.0f);
+            out[0] = a.fs.rho;
+            out[1] = 0.0f;
+            out[2] = 0.0f;
+            out[3] = e_inf;
+            out[4] = e_inf;
+        } else {
+            float s[4];
+#pragma unroll
+            for (int f = 0; f < 4; f++) s[f] = best_gh ? pre_bc(a, best, f) : a.A[f * plane + best];
+            ghost_state(s[0], s[1], s[2], s[3], gi.gx, gi.gy, a.wall, out);
+        }
+#pragma unroll
+        for (int f = 0; f < 5; f++) a.A[f * plane + gi.pidx] = out[f];
+        if (a.cfl) {
+            float uu, vv, pp, TT;
+            prim_from_cons(out[0], out[1], out[2], out[3], out[4], uu, vv, pp, TT);
+            ls = wave_speed(uu, vv, pp, out[0]);
+            if (a.cfl == 2) {
+                float pu, pv, ppp, pT;
+                prim_from_cons(pre_bc(a, gi.pidx, 0), pre_bc(a, gi.pidx, 1), pre_bc(a, gi.pidx, 2),
+                               pre_bc(a, gi.pidx, 3), pre_bc(a, gi.pidx, 4), pu, pv, ppp, pT);
+                ln = sutherland_mu(pT) / (out[0] + 1e-10f);
+            }
+        }
+    }
+    if (a.cfl) block_max2_publish<128>(ls, ln, a.sc->red);
+    if (a.finalize) {
+        __shared__ bool last;
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) last = (atomicAdd(&a.sc->counter, 1u) == gridDim.x - 1);
+        __syncthreads();
+        if (last && threadIdx.x == 0) {
+            __threadfence();
+            finalize_cfl(a);
+        }
+    }
+}
+
+// Phase-1 boundary conditions in place (set-up path).
+__global__ void k_bc_phase1(GridDesc g, float *U, const uint8_t *mask, Freestream fs) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= g.nx || j >= g.ny) return;
+    size_t c = (size_t)j * g.pitch + i;
+    float s[5];
+    for (int k = 0; k < 5; k++) s[k] = U[k * g.plane + c];
+    bc_pointwise(s, mb_type(mask[c]), i, j, g.nx, g.ny, fs);
+    for (int k = 0; k < 5; k++) U[k * g.plane + c] = s[k];
+}
+
+// CFL maxima of a whole state (computeWaveSpeedKernel / computeViscousNumberKernel).
+__global__ void __launch_bounds__(256) k_cfl_state(GridDesc g, const float *U, const uint8_t *mask, DevScalars *sc) {
+    float ls = 0.0f, ln = 0.0f;
+    const long long n = (long long)g.nx * g.ny;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(e / g.nx), i = (int)(e % g.nx);
+        const size_t c = (size_t)j * g.pitch + i;
+        float u, v, p, T;
+        const float rho = U[c];
+        prim_from_cons(rho, U[g.plane + c], U[2 * g.plane + c], U[3 * g.plane + c], U[4 * g.plane + c], u, v, p, T);
+        ls = fmaxf(ls, wave_speed(u, v, p, rho));
+        const float mu = (mb_type(mask[c]) == CT_SOLID) ? 0.0f : sutherland_mu(T);
+        ln = fmaxf(ln, mu / (rho + 1e-10f));
+    }
+    block_max2_publish<256>(ls, ln, sc->red);
+}
+
+__global__ void k_cfl_publish(DevScalars *sc) {
+    sc->cfl[0] = sc->red[0];
+    sc->cfl[1] = sc->red[1];
+    sc->red[0] = 0.0f;
+    sc->red[1] = 0.0f;
+}
+
+// ------------------------------------------------------------ launchers
+size_t stage_smem_bytes(int stage, const StageTune &tn) {
+#define FVM_SZ(NT, K)                                                                              \
+    if (tn.nt == NT && tn.ring == K)                                                               \
+        return stage == 1 ? StageLayout<NT, K, 1>::total : StageLayout<NT, K, 2>::total;
+    FVM_SZ(128, 6) FVM_SZ(128, 8) FVM_SZ(256, 6) FVM_SZ(256, 8)
+#undef FVM_SZ
+    return 0;
+}
+size_t viscous_smem_bytes(const StageTune &tn) {
+    if (tn.nt == 128 && tn.ring == 6) return ViscLayout<128, 6>::total;
+    if (tn.nt == 128 && tn.ring == 8) return ViscLayout<128, 8>::total;
+    if (tn.nt == 256 && tn.ring == 6) return ViscLayout<256, 6>::total;
+    if (tn.nt == 256 && tn.ring == 8) return ViscLayout<256, 8>::total;
+    return 0;
+}
+int stage_cols_per_cta(const StageTune &tn) { return tn.nt - 4; }
+int stage_box_in(const StageTune &) { return kBox; }
+int stage_box_blend(const StageTune &tn) { return tn.nt - 4; }
+
+template <int NT, int K, int STAGE, int SCHEME, int LIM>
+static cudaError_t stage_attr_t() {
+    using L = StageLayout<NT, K, STAGE>;
+    return cudaFuncSetAttribute(k_stage<NT, K, STAGE, SCHEME, LIM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)L::total);
+}
+
+template <int NT, int K>
+static cudaError_t visc_attr_t() {
+    return cudaFuncSetAttribute(k_viscous<NT, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)ViscLayout<NT, K>::total);
+}
+
+template <int NT, int K>
+static cudaError_t prepare_t() {
+    cudaError_t e = cudaSuccess, r;
+#define FVM_A(S, A, B) if ((r = stage_attr_t<NT, K, S, A, B>()) != cudaSuccess) e = r;
+    FVM_A(1, 0, 0) FVM_A(1, 0, 1) FVM_A(1, 1, 0) FVM_A(1, 1, 1)
+    FVM_A(2, 0, 0) FVM_A(2, 0, 1) FVM_A(2, 1, 0) FVM_A(2, 1, 1)
+#undef FVM_A
+    if ((r = visc_attr_t<NT, K>()) != cudaSuccess) e = r;
+    return e;
+}
+
+// Opt the step kernels of a tuning into their dynamic shared memory (done
+// once at set-up, outside any stream capture).
+cudaError_t prepare_step_kernels(const StageTune &tn) {
+    if (tn.nt == 128 && tn.ring == 6) return prepare_t<128, 6>();
+    if (tn.nt == 128 && tn.ring == 8) return prepare_t<128, 8>();
+    if (tn.nt == 256 && tn.ring == 6) return prepare_t<256, 6>();
+    if (tn.nt == 256 && tn.ring == 8) return prepare_t<256, 8>();
+    return cudaErrorInvalidValue;
+}
+
+template <int NT, int K, int STAGE, int SCHEME, int LIM>
+static cudaError_t launch_stage_t(const StageTune &tn, const CUtensorMap &tm_in, const CUtensorMap &tm_blend,
+                                  const StepArgs &a, cudaStream_t st) {
+    using L = StageLayout<NT, K, STAGE>;
+    auto kern = k_stage<NT, K, STAGE, SCHEME, LIM>;
+    dim3 grid((a.g.nx + L::W - 1) / L::W, (a.g.ny + a.rows_per_cta - 1) / a.rows_per_cta);
+    kern<<<grid, NT, L::total, st>>>(tm_in, tm_blend, a);
+    return cudaGetLastError();
+}
+
+template <int NT, int K, int STAGE>
+static cudaError_t launch_stage_s(int scheme, int lim, const StageTune &tn, const CUtensorMap &tm_in,
+                                  const CUtensorMap &tm_blend, const StepArgs &a, cudaStream_t st) {
+    if (scheme == 0 && lim == 0) return launch_stage_t<NT, K, STAGE, 0, 0>(tn, tm_in, tm_blend, a, st);
+    if (scheme == 0 && lim == 1) return launch_stage_t<NT, K, STAGE, 0, 1>(tn, tm_in, tm_blend, a, st);
+    if (scheme == 1 && lim == 0) return launch_stage_t<NT, K, STAGE, 1, 0>(tn, tm_in, tm_blend, a, st);
+    return launch_stage_t<NT, K, STAGE, 1, 1>(tn, tm_in, tm_blend, a, st);
+}
+
+cudaError_t launch_stage(int stage, int scheme, int limiter, const StageTune &tn, const CUtensorMap &tm_in,
+                         const CUtensorMap &tm_blend, const StepArgs &a, cudaStream_t st) {
+#define FVM_ST(NT, K)                                                                                      \
+    if (tn.nt == NT && tn.ring == K)                                                                       \
+        return stage == 1 ? launch_stage_s<NT, K, 1>(scheme, limiter, tn, tm_in, tm_blend, a, st)          \
+                          : launch_stage_s<NT, K, 2>(scheme, limiter, tn, tm_in, tm_blend, a, st);
+    FVM_ST(128, 6) FVM_ST(128, 8) FVM_ST(256, 6) FVM_ST(256, 8)
+#undef FVM_ST
+    return cudaErrorInvalidValue;
+}
+
+template <int NT, int K>
+static cudaError_t launch_viscous_t(const CUtensorMap &tm_in, const StepArgs &a, cudaStream_t st) {
+    using L = ViscLayout<NT, K>;
+    auto kern = k_viscous<NT, K>;
+    dim3 grid((a.g.nx + L::W - 1) / L::W, (a.g.ny + a.rows_per_cta - 1) / a.rows_per_cta);
+    kern<<<grid, NT, L::total, st>>>(tm_in, a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_viscous(const StageTune &tn, const CUtensorMap &tm_in, const StepArgs &a, cudaStream_t st) {
+    if (tn.nt == 128 && tn.ring == 6) return launch_viscous_t<128, 6>(tm_in, a, st);
+    if (tn.nt == 128 && tn.ring == 8) return launch_viscous_t<128, 8>(tm_in, a, st);
+    if (tn.nt == 256 && tn.ring == 6) return launch_viscous_t<256, 6>(tm_in, a, st);
+    if (tn.nt == 256 && tn.ring == 8) return launch_viscous_t<256, 8>(tm_in, a, st);
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_ghost(const GhostArgs &a, cudaStream_t st) {
+    int blocks = (a.n + 127) / 128;
+    if (blocks < 1) blocks = 1;
+    k_ghost<<<blocks, 128, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bc_phase1(const GridDesc &g, float *U, const uint8_t *mask, const Freestream &fs, cudaStream_t st) {
+    dim3 b(32, 8), gr((g.nx + 31) / 32, (g.ny + 7) / 8);
+    k_bc_phase1<<<gr, b, 0, st>>>(g, U, mask, fs);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cfl_state(const GridDesc &g, const float *U, const uint8_t *mask, DevScalars *sc, cudaStream_t st) {
+    long long n = (long long)g.nx * g.ny;
+    int blocks = (int)((n + 255) / 256);
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    k_cfl_state<<<blocks, 256, 0, st>>>(g, U, mask, sc);
+    k_cfl_publish<<<1, 1, 0, st>>>(sc);
+    return cudaGetLastError();
+}
+
+}  // namespace fvm

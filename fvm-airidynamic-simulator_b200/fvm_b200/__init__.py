@@ -1,0 +1,269 @@
+"""fvm_b200 -- Python handle on the B200 compressible-flow hot path.
+
+A thin ctypes layer over the C ABI in include/fvm_b200.h (libfvm_b200.so,
+built in-tree for sm_100a).  `Solver` mirrors the reference's host class
+`CFDSolver` (reference: src/include/solver.cuh:22-257): initialize, reset,
+step, updateObstacleGeometry, computeStableTimeStep, field readback and the
+statistics calls, with the same argument meaning.  Errors raise FvmError
+instead of exiting.  There is no CPU fallback: without the CUDA library or a
+device every call fails.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from .abi import (SimParams, Ext, Diag, KernelTime, STATUS, params_default, compute_derived,
+                  ext_default, workload)
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libfvm_b200.so")
+
+# Every symbol include/fvm_b200.h declares.
+EXPORTS = [
+    "fvm_last_error", "fvm_params_compute_derived", "fvm_params_default", "fvm_ext_default",
+    "fvm_create", "fvm_destroy", "fvm_set_stream", "fvm_initialize", "fvm_resize", "fvm_reset",
+    "fvm_update_obstacle", "fvm_set_ext", "fvm_step", "fvm_steps", "fvm_compute_dt", "fvm_queue_dt",
+    "fvm_read_dt", "fvm_synchronize", "fvm_get_cell_types", "fvm_get_sdf", "fvm_read_fields",
+    "fvm_write_fields", "fvm_read_primitives", "fvm_field_to_device", "fvm_cell_types_to_device",
+    "fvm_vector_arrows", "fvm_max_temperature", "fvm_max_mach", "fvm_memory_usage", "fvm_gpu_mem_info",
+    "fvm_diagnostics", "fvm_shock_standoff", "fvm_set_kernel_timing", "fvm_kernel_times",
+    "fvm_launch_count", "fvm_build_info",
+]
+
+
+class FvmError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"[{STATUS.get(code, code)}] {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def load_library(path=None):
+    """Load libfvm_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = path or LIB_PATH
+    if not os.path.exists(path):
+        raise FvmError(8, f"CUDA library not built: {path} (run __graft_entry__.build())")
+    lib = C.CDLL(path)
+    vp, i, f, sz = C.c_void_p, C.c_int, C.c_float, C.c_size_t
+    fp = C.POINTER(C.c_float)
+    Pp = C.POINTER(SimParams)
+    lib.fvm_last_error.restype = C.c_char_p
+    lib.fvm_build_info.restype = C.c_char_p
+    lib.fvm_params_default.argtypes = [Pp]
+    lib.fvm_params_default.restype = None
+    lib.fvm_params_compute_derived.argtypes = [Pp]
+    lib.fvm_params_compute_derived.restype = None
+    lib.fvm_ext_default.argtypes = [C.POINTER(Ext)]
+    lib.fvm_ext_default.restype = None
+    lib.fvm_create.argtypes = [C.POINTER(vp)]
+    lib.fvm_destroy.argtypes = [vp]
+    lib.fvm_set_stream.argtypes = [vp, vp]
+    lib.fvm_initialize.argtypes = [vp, Pp, C.POINTER(Ext)]
+    lib.fvm_resize.argtypes = [vp, i, i]
+    lib.fvm_reset.argtypes = [vp, Pp]
+    lib.fvm_update_obstacle.argtypes = [vp, Pp]
+    lib.fvm_set_ext.argtypes = [vp, C.POINTER(Ext)]
+    lib.fvm_step.argtypes = [vp, Pp]
+    lib.fvm_steps.argtypes = [vp, Pp, i]
+    lib.fvm_compute_dt.argtypes = [vp, Pp, fp]
+    lib.fvm_queue_dt.argtypes = [vp, Pp]
+    lib.fvm_read_dt.argtypes = [vp, Pp, fp]
+    lib.fvm_synchronize.argtypes = [vp]
+    lib.fvm_get_cell_types.argtypes = [vp, vp]
+    lib.fvm_get_sdf.argtypes = [vp, vp]
+    lib.fvm_read_fields.argtypes = [vp] + [vp] * 5
+    lib.fvm_write_fields.argtypes = [vp] + [vp] * 5
+    lib.fvm_read_primitives.argtypes = [vp] + [vp] * 4
+    lib.fvm_field_to_device.argtypes = [vp, i, vp]
+    lib.fvm_cell_types_to_device.argtypes = [vp, vp]
+    lib.fvm_vector_arrows.argtypes = [vp, vp, i, i, f, f, f, f, C.POINTER(i)]
+    lib.fvm_max_temperature.argtypes = [vp, fp]
+    lib.fvm_max_mach.argtypes = [vp, fp]
+    lib.fvm_memory_usage.argtypes = [vp, C.POINTER(sz)]
+    lib.fvm_gpu_mem_info.argtypes = [C.POINTER(sz), C.POINTER(sz)]
+    lib.fvm_diagnostics.argtypes = [vp, C.POINTER(Diag)]
+    lib.fvm_shock_standoff.argtypes = [vp, C.POINTER(C.c_double)]
+    lib.fvm_set_kernel_timing.argtypes = [vp, i]
+    lib.fvm_kernel_times.argtypes = [vp, C.POINTER(KernelTime), i, C.POINTER(i)]
+    lib.fvm_launch_count.argtypes = [vp, C.POINTER(C.c_longlong)]
+    _lib = lib
+    return lib
+
+
+def _check(rc):
+    if rc != 0:
+        raise FvmError(rc, _lib.fvm_last_error().decode(errors="replace"))
+
+
+def _p(a):
+    return C.c_void_p(a.ctypes.data) if a is not None else None
+
+
+class Solver:
+    """One solve on the GPU (the reference CFDSolver's public surface)."""
+
+    def __init__(self, params=None, ext=None):
+        self.lib = load_library()
+        h = C.c_void_p()
+        _check(self.lib.fvm_create(C.byref(h)))
+        self.h = h
+        self.params = None
+        self.ext = None
+        if params is not None:
+            self.initialize(params, ext)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.fvm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # lifecycle -----------------------------------------------------------
+    def initialize(self, params, ext=None):
+        self.params = params
+        self.ext = ext if ext is not None else ext_default()
+        _check(self.lib.fvm_initialize(self.h, C.byref(self.params), C.byref(self.ext)))
+
+    def reset(self, params=None):
+        if params is not None:
+            self.params = params
+        _check(self.lib.fvm_reset(self.h, C.byref(self.params)))
+
+    def resize(self, nx, ny):
+        _check(self.lib.fvm_resize(self.h, int(nx), int(ny)))
+
+    def update_obstacle(self, params):
+        self.params = params
+        _check(self.lib.fvm_update_obstacle(self.h, C.byref(self.params)))
+
+    def set_ext(self, ext):
+        self.ext = ext
+        _check(self.lib.fvm_set_ext(self.h, C.byref(self.ext)))
+
+    def set_stream(self, stream_handle):
+        _check(self.lib.fvm_set_stream(self.h, C.c_void_p(stream_handle) if stream_handle else None))
+
+    # stepping --------------------------------------------------------------
+    def step(self, n=1):
+        _check(self.lib.fvm_steps(self.h, C.byref(self.params), int(n)))
+
+    def compute_dt(self):
+        dt = C.c_float()
+        _check(self.lib.fvm_compute_dt(self.h, C.byref(self.params), C.byref(dt)))
+        return dt.value
+
+    def synchronize(self):
+        _check(self.lib.fvm_synchronize(self.h))
+
+    @property
+    def shape(self):
+        return (self.params.ny, self.params.nx)
+
+    # readback --------------------------------------------------------------
+    def fields(self):
+        n = self.params.nx * self.params.ny
+        out = [np.empty(n, np.float32) for _ in range(5)]
+        _check(self.lib.fvm_read_fields(self.h, *[_p(a) for a in out]))
+        return np.stack([a.reshape(self.shape) for a in out])
+
+    def write_fields(self, U):
+        U = [np.ascontiguousarray(U[k], dtype=np.float32).reshape(-1) for k in range(5)]
+        _check(self.lib.fvm_write_fields(self.h, *[_p(a) for a in U]))
+
+    def primitives(self):
+        n = self.params.nx * self.params.ny
+        out = [np.empty(n, np.float32) for _ in range(4)]
+        _check(self.lib.fvm_read_primitives(self.h, *[_p(a) for a in out]))
+        return np.stack([a.reshape(self.shape) for a in out])
+
+    def cell_types(self):
+        out = np.empty(self.params.nx * self.params.ny, np.uint8)
+        _check(self.lib.fvm_get_cell_types(self.h, _p(out)))
+        return out.reshape(self.shape)
+
+    def sdf(self):
+        out = np.empty(self.params.nx * self.params.ny, np.float32)
+        _check(self.lib.fvm_get_sdf(self.h, _p(out)))
+        return out.reshape(self.shape)
+
+    def field_to_device(self, kind, dev_ptr):
+        _check(self.lib.fvm_field_to_device(self.h, int(kind), C.c_void_p(dev_ptr)))
+
+    def cell_types_to_device(self, dev_ptr):
+        _check(self.lib.fvm_cell_types_to_device(self.h, C.c_void_p(dev_ptr)))
+
+    def vector_arrows(self, dev_ptr, max_vertices, step, u_inf, max_len, head_angle, head_len):
+        n = C.c_int()
+        _check(self.lib.fvm_vector_arrows(self.h, C.c_void_p(dev_ptr), int(max_vertices), int(step),
+                                          float(u_inf), float(max_len), float(head_angle), float(head_len),
+                                          C.byref(n)))
+        return n.value
+
+    # statistics / diagnostics -------------------------------------------
+    def max_temperature(self):
+        v = C.c_float()
+        _check(self.lib.fvm_max_temperature(self.h, C.byref(v)))
+        return v.value
+
+    def max_mach(self):
+        v = C.c_float()
+        _check(self.lib.fvm_max_mach(self.h, C.byref(v)))
+        return v.value
+
+    def memory_usage(self):
+        v = C.c_size_t()
+        _check(self.lib.fvm_memory_usage(self.h, C.byref(v)))
+        return v.value
+
+    def diagnostics(self):
+        d = Diag()
+        _check(self.lib.fvm_diagnostics(self.h, C.byref(d)))
+        return d
+
+    def shock_standoff(self):
+        v = C.c_double()
+        _check(self.lib.fvm_shock_standoff(self.h, C.byref(v)))
+        return v.value
+
+    def set_kernel_timing(self, on):
+        _check(self.lib.fvm_set_kernel_timing(self.h, 1 if on else 0))
+
+    def kernel_times(self):
+        cap = 32
+        arr = (KernelTime * cap)()
+        n = C.c_int()
+        _check(self.lib.fvm_kernel_times(self.h, arr, cap, C.byref(n)))
+        return {arr[k].name.decode(): (arr[k].launches, arr[k].total_ms) for k in range(min(n.value, cap))}
+
+    def launch_count(self):
+        v = C.c_longlong()
+        _check(self.lib.fvm_launch_count(self.h, C.byref(v)))
+        return v.value
+
+
+def gpu_mem_info():
+    lib = load_library()
+    f, t = C.c_size_t(), C.c_size_t()
+    _check(lib.fvm_gpu_mem_info(C.byref(f), C.byref(t)))
+    return f.value, t.value
+
+
+__all__ = ["Solver", "FvmError", "SimParams", "Ext", "Diag", "params_default", "compute_derived",
+           "ext_default", "workload", "load_library", "gpu_mem_info", "EXPORTS", "LIB_PATH"]

@@ -1,0 +1,234 @@
+/*
+ * fvm_b200.h -- C ABI of the B200 (sm_100a) compressible-flow hot path.
+ *
+ * This library replaces the device side of the reference solver class
+ * `CFDSolver` (reference: src/include/solver.cuh:22-257, implemented in
+ * src/solver.cu:2873-3845).  Every entry point returns an int status
+ * (FVM_OK == 0) instead of calling exit() the way the reference's CUDA_CHECK
+ * macro does (src/include/solver.cuh:8-19).  Signatures use plain pointers and
+ * sizes only.  A handle owns one CUDA stream and every device buffer of one
+ * solve; calls on one handle must be serialised by the caller, exactly like
+ * the reference protocol (one solver thread, src/main.cpp:225-380).
+ *
+ * Field layout seen through this ABI (readback/writeback) is the reference's:
+ * row-major, idx = j*nx + i, SoA float arrays of length nx*ny.
+ */
+#ifndef FVM_B200_H
+#define FVM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include <stdbool.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+enum fvm_status {
+    FVM_OK = 0,
+    FVM_ERR_INVALID = 1,      /* bad argument (null pointer, nx<=0, unknown enum, ...) */
+    FVM_ERR_CUDA = 2,         /* a CUDA runtime/driver call failed */
+    FVM_ERR_ALLOC = 3,        /* device or pinned allocation failed */
+    FVM_ERR_STATE = 4,        /* call out of order (e.g. step before initialize) */
+    FVM_ERR_TIMEOUT = 5,      /* a bounded device wait gave up (kernel error word set) */
+    FVM_ERR_NONFINITE = 6,    /* device non-finite counter tripped */
+    FVM_ERR_BUDGET = 7,       /* batch/serve admission refused: over HBM budget */
+    FVM_ERR_UNSUPPORTED = 8   /* feature not available on this device */
+};
+
+/* Text of the last error recorded on the calling thread (never NULL). */
+const char *fvm_last_error(void);
+
+/* ------------------------------------------------------------ parameters */
+/* Obstacle shapes.  0..5 are the reference enum `ObstacleShape`
+ * (src/include/common.h:39-47); 6 is a blunted cone (sphere-cone) with no
+ * reference counterpart. */
+enum fvm_shape {
+    FVM_SHAPE_CIRCLE = 0,
+    FVM_SHAPE_STAR = 1,
+    FVM_SHAPE_DIAMOND = 2,
+    FVM_SHAPE_CAPSULE = 3,
+    FVM_SHAPE_TRIANGLE = 4,
+    FVM_SHAPE_STARSHIP = 5,
+    FVM_SHAPE_CONE_CAPSULE = 6
+};
+
+/* Cell classes, values of the reference enum `CellType` (src/include/common.h:105-111). */
+enum fvm_cell_type {
+    FVM_CELL_FLUID = 0,
+    FVM_CELL_SOLID = 1,
+    FVM_CELL_GHOST = 2,
+    FVM_CELL_INFLOW = 3,
+    FVM_CELL_OUTFLOW = 4
+};
+
+/* Byte-for-byte the reference `struct SimParams` (src/include/common.h:50-102):
+ * 112 bytes, 4-byte aligned, same field order.  The C++ shim static_asserts the
+ * equivalence so `SimParams*` can be passed straight through. */
+typedef struct fvm_sim_params {
+    int nx, ny;
+    float dx, dy;
+    float domain_width, domain_height;
+    float mach, T_inf, p_inf, rho_inf, u_inf, v_inf, c_inf;
+    float obstacle_x, obstacle_y, obstacle_r, obstacle_rotation;
+    int obstacle_shape;
+    float wing_rotation;
+    float cfl, dt, t_current;
+    int step;
+    bool enable_viscosity;
+    float cfl_visc;
+    bool adiabatic_wall;
+    float T_wall;
+    bool paused;
+} fvm_sim_params;
+
+/* Host-side `SimParams::computeDerived` (src/include/common.h:93-101):
+ * rho_inf, c_inf, u_inf, dx, dy and obstacle_y = domain_height/2. */
+void fvm_params_compute_derived(fvm_sim_params *p);
+/* The reference's default member initialisers (src/include/common.h:53-90). */
+void fvm_params_default(fvm_sim_params *p);
+
+enum fvm_flux_scheme { FVM_FLUX_HLLC = 0, FVM_FLUX_AUSM_PLUS = 1 };
+enum fvm_limiter { FVM_LIMITER_MINMOD = 0, FVM_LIMITER_VAN_LEER = 1 };
+enum fvm_dt_policy {
+    FVM_DT_FIXED = 0,     /* use SimParams.dt as given (reference KernelBenchmark) */
+    FVM_DT_RECOMPUTE = 1  /* dt of step n+1 from the CFL reduction fused into step n */
+};
+
+/* Knobs the reference hard-codes.  fvm_ext_default() reproduces the reference:
+ * HLLC (src/solver.cu:1572,1658), minmod (src/solver.cu:110-150), Pr 0.71
+ * (src/include/common.h:19), fixed dt. */
+typedef struct fvm_ext {
+    int flux_scheme;        /* enum fvm_flux_scheme */
+    int limiter;            /* enum fvm_limiter */
+    float prandtl;          /* 0.71 in the reference */
+    int dt_policy;          /* enum fvm_dt_policy */
+    float cone_half_angle;  /* FVM_SHAPE_CONE_CAPSULE: frustum half angle [rad] */
+    float cone_length;      /* FVM_SHAPE_CONE_CAPSULE: frustum length along the axis [m] */
+    float ref_length;       /* reference length for force coefficients [m] (0: 2*obstacle_r) */
+    int reserved[8];
+} fvm_ext;
+
+void fvm_ext_default(fvm_ext *e);
+
+/* ------------------------------------------------------------- lifecycle */
+typedef struct fvm_handle fvm_handle;
+
+int fvm_create(fvm_handle **out);
+int fvm_destroy(fvm_handle *h);
+
+/* Launch this handle's work on `stream` (a cudaStream_t); NULL restores the
+ * handle's own stream.  The caller keeps ownership of the stream. */
+int fvm_set_stream(fvm_handle *h, void *stream);
+
+/* CFDSolver::initialize (src/solver.cu:3102-3111): allocate for nx*ny, then reset. */
+int fvm_initialize(fvm_handle *h, const fvm_sim_params *p, const fvm_ext *ext);
+/* CFDSolver::resize (src/solver.cu:3119-3129). */
+int fvm_resize(fvm_handle *h, int nx, int ny);
+/* CFDSolver::reset (src/solver.cu:3136-3162): freestream, SDF + cell marking,
+ * boundary conditions, primitives, viscosity field. */
+int fvm_reset(fvm_handle *h, const fvm_sim_params *p);
+/* CFDSolver::updateObstacleGeometry (src/solver.cu:3171-3196). */
+int fvm_update_obstacle(fvm_handle *h, const fvm_sim_params *p);
+/* Replace the extension knobs without touching the flow state. */
+int fvm_set_ext(fvm_handle *h, const fvm_ext *ext);
+
+/* -------------------------------------------------------------- stepping */
+/* CFDSolver::step (src/solver.cu:3289-3412): one SSP-RK2 step (Strang split
+ * when p->enable_viscosity); advances p->t_current and p->step.  Under
+ * FVM_DT_RECOMPUTE, p->dt receives the dt that was used. */
+int fvm_step(fvm_handle *h, fvm_sim_params *p);
+/* n steps back to back (graph-captured after the first call for a given shape). */
+int fvm_steps(fvm_handle *h, fvm_sim_params *p, int n);
+/* CFDSolver::computeStableTimeStep (src/solver.cu:3273-3278). */
+int fvm_compute_dt(fvm_handle *h, const fvm_sim_params *p, float *dt_out);
+/* CFDSolver::queueTimeStepComputation / readTimeStepResult (src/solver.cu:3206-3265). */
+int fvm_queue_dt(fvm_handle *h, const fvm_sim_params *p);
+int fvm_read_dt(fvm_handle *h, const fvm_sim_params *p, float *dt_out);
+/* Block until this handle's stream is idle; reports a device error word. */
+int fvm_synchronize(fvm_handle *h);
+
+/* -------------------------------------------------------------- readback */
+/* CFDSolver::getCellTypes (src/solver.cu:3432-3435). */
+int fvm_get_cell_types(fvm_handle *h, uint8_t *host_types);
+/* The signed-distance field, nx*ny floats (no reference accessor). */
+int fvm_get_sdf(fvm_handle *h, float *host_sdf);
+/* Conserved fields to/from host SoA buffers (the reference has no accessor;
+ * its private d_rho_ ... d_rho_e_, src/include/solver.cuh:92-96).  Any pointer
+ * may be NULL to skip that field.  fvm_write_fields recomputes primitives. */
+int fvm_read_fields(fvm_handle *h, float *rho, float *rho_u, float *rho_v, float *E, float *rho_e);
+int fvm_write_fields(fvm_handle *h, const float *rho, const float *rho_u, const float *rho_v,
+                     const float *E, const float *rho_e);
+/* Primitive fields u, v, p, T as left by the last step/reset (host). */
+int fvm_read_primitives(fvm_handle *h, float *u, float *v, float *p, float *T);
+
+/* Derived field into a device pointer (CFDSolver::compute*ToDevice,
+ * src/solver.cu:3632-3671); kinds follow the reference's field selector. */
+enum fvm_field_kind {
+    FVM_FIELD_TEMPERATURE = 0,
+    FVM_FIELD_PRESSURE = 1,
+    FVM_FIELD_DENSITY = 2,
+    FVM_FIELD_VELOCITY_MAG = 3,
+    FVM_FIELD_MACH = 4
+};
+int fvm_field_to_device(fvm_handle *h, int kind, float *dev_dst);
+/* CFDSolver::convertCellTypesToDevice (src/solver.cu:3452-3459). */
+int fvm_cell_types_to_device(fvm_handle *h, float *dev_dst);
+/* CFDSolver::generateVectorArrows (src/solver.cu:3809-3845); *n_vertices_out
+ * receives the vertex count (the reference's return value). */
+int fvm_vector_arrows(fvm_handle *h, float *dev_vertex_data, int max_vertices, int step,
+                      float u_inf, float max_arrow_length, float arrow_head_angle,
+                      float arrow_head_length, int *n_vertices_out);
+
+/* ----------------------------------------------------------------- stats */
+/* CFDSolver::getMaxTemperature / getMaxMach (src/solver.cu:3417-3426). */
+int fvm_max_temperature(fvm_handle *h, float *out);
+int fvm_max_mach(fvm_handle *h, float *out);
+/* CFDSolver::getSimulationMemoryUsage (src/solver.cu:3474-3514): bytes this handle holds. */
+int fvm_memory_usage(fvm_handle *h, size_t *bytes);
+/* CFDSolver::getGPUMemoryInfo (src/solver.cu:3468-3471): (free, total), the
+ * implementation's positional order. */
+int fvm_gpu_mem_info(size_t *free_bytes, size_t *total_bytes);
+
+/* FP64 diagnostics reduced on the device (no reference counterpart).
+ * Forces act on the obstacle per unit span; coefficients use
+ * q_inf = 0.5*rho_inf*u_inf^2 and ref_length. */
+typedef struct fvm_diag {
+    double force_x, force_y;      /* pressure + viscous wall force [N/m] */
+    double cd, cl;                /* force coefficients */
+    double mass, mom_x, mom_y, energy;   /* totals over non-solid cells [per m span] */
+    double wall_heat;             /* integrated wall heat flux into the wall [W/m] */
+    double wall_heat_max;         /* peak wall heat flux [W/m^2] */
+    double reserved[6];
+} fvm_diag;
+int fvm_diagnostics(fvm_handle *h, fvm_diag *out);
+
+/* Shock standoff along row j = ny/2: distance between the shock (pressure
+ * crossing halfway from p_inf to the normal-shock pressure) and the obstacle
+ * surface (sdf zero crossing), both upstream of the obstacle [m]. */
+int fvm_shock_standoff(fvm_handle *h, double *standoff_out);
+
+/* Kernel time accounting for measurement: when enabled, each launch on the
+ * handle's stream is bracketed by CUDA events.  fvm_kernel_times fills up to
+ * `cap` entries {name, launches, total_ms} for kernels launched since the
+ * last reset of the counters. */
+typedef struct fvm_kernel_time {
+    char name[48];
+    long long launches;
+    double total_ms;
+} fvm_kernel_time;
+int fvm_set_kernel_timing(fvm_handle *h, int enable);
+int fvm_kernel_times(fvm_handle *h, fvm_kernel_time *out, int cap, int *count_out);
+
+/* Count of kernels this library launched on the handle since creation. */
+int fvm_launch_count(fvm_handle *h, long long *count_out);
+
+/* Library build description (arch, flags). */
+const char *fvm_build_info(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FVM_B200_H */

@@ -1,0 +1,163 @@
+"""Parity of the CUDA library (through the C ABI) with the oracle.
+
+Checks, on seeded small grids the CPU oracle finishes in seconds:
+  * masks and SDF: bit-exact against the reference's own FP32 CUDA kernel
+    (oracle/_ref), and against the FP32 oracle except at tie cells;
+  * initial state after reset;
+  * conserved fields after 1, 10 and 100 steps against the FP32 oracle run on
+    the same geometry and start state; tolerances (vs the FP32 oracle):
+      smooth flow  relative L-inf <= 1e-5
+      shocks       relative L1    <= 1e-4 (L-inf away from walls reported)
+  * the same against the reference's FP32 CUDA solver (oracle/_ref).
+"""
+import numpy as np
+import pytest
+
+from helpers import small, rel_l1, rel_linf, away_from_walls, FIELDS
+
+pytestmark = pytest.mark.gpu
+
+from fvm_b200 import Solver, abi  # noqa: E402
+from oracle.oracle import Oracle  # noqa: E402
+from oracle import ref as refmod  # noqa: E402
+
+CASES = {
+    # name: (workload, nx, ny, overrides, smooth)
+    "euler_m3_circle": ("euler_m3_circle", 256, 128, {}, False),
+    "euler_m3_star": ("euler_m3_circle", 192, 96, {"obstacle_shape": abi.SHAPE_STAR, "obstacle_r": 0.15,
+                                                   "obstacle_rotation": 0.3}, False),
+    "ns_karman": ("ns_karman_re200", 256, 128, {}, True),
+    "ns_cone_m8": ("ns_hypersonic_cone", 256, 128, {}, False),
+    "ref_bench": ("reference_benchmark", 200, 100, {}, False),
+    "euler_ausm": ("euler_m3_circle", 160, 80, {"flux_scheme": abi.FLUX_AUSM_PLUS}, False),
+    "euler_vanleer": ("euler_m3_circle", 160, 80, {"limiter": abi.LIMITER_VAN_LEER}, False),
+    "ns_diamond_iso": ("ns_karman_re200", 130, 70, {"obstacle_shape": abi.SHAPE_DIAMOND, "adiabatic_wall": False,
+                                                    "T_wall": 350.0, "obstacle_rotation": 0.5}, True),
+}
+
+
+def _pair(case, bits=32):
+    name, nx, ny, kw, smooth = CASES[case]
+    p, e = small(name, nx, ny, **kw)
+    s = Solver(p, e)
+    o = Oracle(p, e, bits=bits)
+    o.set_geometry(s.sdf(), s.cell_types())
+    o.set_fields(s.fields())
+    return s, o, p, e, smooth
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_reset_state_matches_oracle(case):
+    name, nx, ny, kw, _ = CASES[case]
+    p, e = small(name, nx, ny, **kw)
+    s = Solver(p, e)
+    o = Oracle(p, e, bits=32)
+    o.set_geometry(s.sdf(), s.cell_types())
+    o.reinit()
+    U = s.fields()
+    R = o.fields()
+    assert np.isfinite(U).all()
+    err = rel_linf(U, R)
+    assert err.max() <= 2e-6, dict(zip(FIELDS, err))
+
+
+@pytest.mark.parametrize("case", list(CASES))
+@pytest.mark.parametrize("steps", [1, 10, 100])
+def test_steps_match_fp32_oracle(case, steps):
+    s, o, p, e, smooth = _pair(case)
+    dt = o.compute_dt()
+    p.dt = dt
+    s.step(steps)
+    for _ in range(steps):
+        o.step(dt)
+    U, R = s.fields(), o.fields()
+    assert np.isfinite(U).all()
+    l1 = rel_l1(U, R)
+    linf = rel_linf(U, R)
+    far = away_from_walls(s.cell_types(), 3)
+    linf_far = rel_linf(U, R, far)
+    msg = {"l1": dict(zip(FIELDS, l1)), "linf": dict(zip(FIELDS, linf)), "linf_far": dict(zip(FIELDS, linf_far))}
+    if smooth:
+        assert linf.max() <= 1e-5, msg
+    assert l1.max() <= 1e-4, msg
+
+
+@pytest.mark.parametrize("case", ["euler_m3_circle", "ns_karman"])
+def test_recompute_dt_policy_matches_oracle(case):
+    s, o, p, e, smooth = _pair(case)
+    e.dt_policy = abi.DT_RECOMPUTE
+    s.set_ext(e)
+    steps = 20
+    s.step(steps)
+    dts = []
+    for _ in range(steps):
+        dt = o.compute_dt()
+        dts.append(dt)
+        o.step(dt)
+    assert abs(p.dt - dts[-1]) <= 1e-6 * dts[-1], (p.dt, dts[-1])
+    assert abs(p.t_current - sum(dts)) <= 1e-5 * sum(dts)
+    U, R = s.fields(), o.fields()
+    assert rel_l1(U, R).max() <= 1e-4
+
+
+def test_step_fp64_error_is_stated():
+    """The FP32 device result against the FP64 oracle after 100 steps on the
+    Mach-3 circle: relative L1 stays at FP32 rounding level."""
+    s, o, p, e, _ = _pair("euler_m3_circle", bits=64)
+    dt = o.compute_dt()
+    p.dt = dt
+    s.step(100)
+    for _ in range(100):
+        o.step(dt)
+    l1 = rel_l1(s.fields(), o.fields())
+    assert l1.max() <= 1e-4, dict(zip(FIELDS, l1))
+
+
+# ------------------------------------------------ against the reference CUDA
+needs_ref = pytest.mark.skipif(not refmod.available(), reason="oracle/_ref not built")
+
+REF_CASES = ["euler_m3_circle", "euler_m3_star", "ns_karman", "ref_bench", "ns_cone_m8"]
+
+
+@needs_ref
+@pytest.mark.parametrize("case", REF_CASES + ["diamond", "capsule", "triangle", "starship"])
+def test_masks_bit_exact_vs_reference(case):
+    if case in CASES:
+        name, nx, ny, kw, _ = CASES[case]
+    else:
+        shape = {"diamond": abi.SHAPE_DIAMOND, "capsule": abi.SHAPE_CAPSULE, "triangle": abi.SHAPE_TRIANGLE,
+                 "starship": abi.SHAPE_STARSHIP}[case]
+        name, nx, ny, kw = "euler_m3_circle", 301, 157, {"obstacle_shape": shape, "obstacle_r": 0.17,
+                                                         "obstacle_rotation": 0.7, "wing_rotation": 0.4}
+    p, e = small(name, nx, ny, **kw)
+    if p.obstacle_shape == abi.SHAPE_CONE_CAPSULE:
+        pytest.skip("blunted cone has no reference counterpart")
+    s = Solver(p, e)
+    r = refmod.RefSolver(p)
+    rsdf, rct = r.geometry()
+    assert np.array_equal(s.cell_types(), rct)
+    assert np.array_equal(s.sdf().view(np.uint32), rsdf.view(np.uint32))
+
+
+@needs_ref
+@pytest.mark.parametrize("case", REF_CASES)
+def test_steps_match_reference_cuda(case):
+    name, nx, ny, kw, smooth = CASES[case]
+    if abi.workload(name)[0].obstacle_shape == abi.SHAPE_CONE_CAPSULE or kw.get("flux_scheme") or kw.get("limiter"):
+        pytest.skip("no reference counterpart")
+    p, e = small(name, nx, ny, **kw)
+    r = refmod.RefSolver(p)
+    s = Solver(p, e)
+    s.write_fields(r.fields())
+    dt = r.compute_dt()
+    p.dt = dt
+    r.steps(100, dt=dt)
+    s.step(100)
+    U, R = s.fields(), r.fields()
+    far = away_from_walls(s.cell_types(), 3)
+    l1 = rel_l1(U, R)
+    linf_far = rel_linf(U, R, far)
+    msg = {"l1": dict(zip(FIELDS, l1)), "linf_far": dict(zip(FIELDS, linf_far))}
+    if smooth:
+        assert linf_far.max() <= 1e-5, msg
+    assert l1.max() <= 1e-4, msg

@@ -990,6 +990,37 @@ extern "C" int fvm_launch_count(fvm_handle *h, long long *count_out) {
     return FVM_OK;
 }
 
+extern "C" int fvm_debug_stage1(fvm_handle *h, float dt, int with_ghost, float *rho, float *rho_u, float *rho_v,
+                                float *E, float *rho_e) {
+    CHECK_INIT(h);
+    k_set_scalars<<<1, 1, 0, h->stream>>>(h->sc, dt, 0.0f, 0);
+    CK(cudaGetLastError());
+    float *Un = h->buf[BUF_N], *Us = h->buf[BUF_S];
+    StepArgs a1 = step_args(h, Us, 1, 0, 1.0f);
+    CK(launch_stage(1, h->ext.flux_scheme, h->ext.limiter, h->tune, h->tm_in[BUF_N], h->tm_ctr[BUF_N], a1, h->stream));
+    if (with_ghost && h->n_ghost > 0) {
+        GhostArgs g1 = ghost_args(h, Us, Un, nullptr, 0, 0);
+        CK(launch_ghost(g1, h->stream));
+    }
+    float *dst[5] = {rho, rho_u, rho_v, E, rho_e};
+    for (int k = 0; k < 5; k++)
+        if (dst[k])
+            CK(cudaMemcpy2DAsync(dst[k], (size_t)h->g.nx * 4, Us + (size_t)k * h->g.plane, (size_t)h->g.pitch * 4,
+                                 (size_t)h->g.nx * 4, h->g.ny, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->dt_ready = false;
+    return check_device_error(h);
+}
+
+extern "C" int fvm_debug_ghost_table(fvm_handle *h, int *out, int cap, int *count_out) {
+    CHECK_INIT(h);
+    static_assert(sizeof(GhostInfo) == 7 * sizeof(int), "GhostInfo layout");
+    if (count_out) *count_out = h->n_ghost;
+    int n = std::min(cap, h->n_ghost);
+    if (out && n > 0) CK(cudaMemcpy(out, h->ghosts, (size_t)n * sizeof(GhostInfo), cudaMemcpyDeviceToHost));
+    return FVM_OK;
+}
+
 extern "C" const char *fvm_build_info(void) {
     return "fvm_b200: sm_100a, nvcc " FVM_STR(__CUDACC_VER_MAJOR__) "." FVM_STR(__CUDACC_VER_MINOR__)
            ", --use_fast_math, marching TMA stage kernels";

@@ -261,8 +261,6 @@ __global__ void k_mask(GridDesc g, const uint8_t *ct, uint8_t *mask) {
     mask[(size_t)j * g.pitch + i] = (uint8_t)m;
 }
 
-__constant__ int c_nb[8][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}, {-1, -1}, {1, -1}, {-1, 1}, {1, 1}};
-
 // Ghost-cell table: count pass (list == nullptr) or fill pass.
 // Normal and neighbour dot products use the reference's expressions
 // (src/solver.cu:2054-2098); a candidate must have sdf > 0 and dot > -1 (the
@@ -290,12 +288,14 @@ __global__ void k_ghost_table(GridDesc g, const float *sdf, const uint8_t *ct, G
     int codes[8];
     int n = 0;
     for (int k = 0; k < 8; k++) {
-        int ni = i + c_nb[k][0], nj = j + c_nb[k][1];
+        int di, dj;
+        ghost_neighbour(k, di, dj);
+        int ni = i + di, nj = j + dj;
         if (ni < 0 || ni >= nx || nj < 0 || nj >= ny) continue;
         size_t q = (size_t)nj * g.pitch + ni;
         if (!(sdf[q] > 0.0f)) continue;
-        float dir_x = (float)c_nb[k][0];
-        float dir_y = (float)c_nb[k][1];
+        float dir_x = (float)di;
+        float dir_y = (float)dj;
         float len = sqrtf(dir_x * dir_x + dir_y * dir_y);
         float dot = (dir_x * gx + dir_y * gy) / len;
         if (!(dot > -1.0f)) continue;

@@ -375,6 +375,22 @@ struct Freestream {
     float rho, u, v, p;
 };
 
+// Neighbour k of the ghost-cell search in the reference's order
+// {(-1,0),(1,0),(0,-1),(0,1),(-1,-1),(1,-1),(-1,1),(1,1)} (src/solver.cu:2072),
+// computed arithmetically (no constant-memory table).
+__host__ __device__ __forceinline__ void ghost_neighbour(int k, int &di, int &dj) {
+    if (k < 2) {
+        di = (k == 0) ? -1 : 1;
+        dj = 0;
+    } else if (k < 4) {
+        di = 0;
+        dj = (k == 2) ? -1 : 1;
+    } else {
+        di = (k & 1) ? 1 : -1;
+        dj = (k < 6) ? -1 : 1;
+    }
+}
+
 // Phase 1 of applyBoundaryConditionsKernel (src/solver.cu:1905-2042) for a
 // non-ghost cell: inflow, right-outflow NRBC, bottom/top NRBC, solid.
 // U is updated in place.  Ghost cells are left for the ghost pass.

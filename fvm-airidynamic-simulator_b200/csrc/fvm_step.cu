@@ -53,13 +53,24 @@ __device__ __forceinline__ void block_max2_publish(float a, float b, float *dst)
 // elements per dimension; 132 floats = 528 B keeps every box start 16-byte
 // aligned).  A staged row is NB boxes, each stored as [field][kBox].
 constexpr int kBox = 132;
+// TMA tensor-copy destinations must be 128-byte aligned: each staged box
+// ([5][kBox] floats = 2640 B) occupies a 2688-byte (672-float) stride.
+constexpr int kBoxStride = 672;
+constexpr size_t align128(size_t b) { return (b + 127) & ~(size_t)127; }
 
 // Address of (field f, staged column x) in a ring slot of NB boxes.
 template <int NB>
 __device__ __forceinline__ float ring_at(const float *slot_base, int f, int x) {
     if (NB == 1) return slot_base[f * kBox + x];
     const int b = x / kBox;
-    return slot_base[(b * 5 + f) * kBox + (x - b * kBox)];
+    return slot_base[b * kBoxStride + f * kBox + (x - b * kBox)];
+}
+
+// Dynamic shared memory rounded up to a 128-byte boundary (the launch asks
+// for 128 extra bytes).
+__device__ __forceinline__ unsigned char *aligned_smem(unsigned char *p) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    return reinterpret_cast<unsigned char *>((a + 127) & ~(uintptr_t)127);
 }
 
 template <int NT, int K, int STAGE>
@@ -70,10 +81,12 @@ struct StageLayout {
     static constexpr int PR = 5;       // primitive / mask ring (rows)
     static constexpr int XR = 3;       // x-face ring
     static constexpr int YR = 2;       // y-face ring
+    static constexpr int SLOT = NB * kBoxStride;                       // floats per input slot
+    static constexpr int BSLOT = (int)(align128((size_t)5 * W * 4) / 4);  // floats per blend slot
     static constexpr size_t raw_off = 0;
-    static constexpr size_t raw_bytes = (size_t)K * 5 * BW * 4;
+    static constexpr size_t raw_bytes = (size_t)K * SLOT * 4;
     static constexpr size_t bl_off = raw_off + raw_bytes;
-    static constexpr size_t bl_bytes = STAGE == 2 ? (size_t)K * 5 * W * 4 : 0;
+    static constexpr size_t bl_bytes = STAGE == 2 ? (size_t)K * BSLOT * 4 : 0;
     static constexpr size_t p_off = bl_off + bl_bytes;
     static constexpr size_t p_bytes = (size_t)PR * NT * 16;
     static constexpr size_t x_off = p_off + p_bytes;
@@ -83,7 +96,7 @@ struct StageLayout {
     static constexpr size_t m_off = y_off + y_bytes;
     static constexpr size_t m_bytes = (size_t)PR * NT;
     static constexpr size_t bar_off = (m_off + m_bytes + 15) & ~(size_t)15;
-    static constexpr size_t total = bar_off + K * 8;
+    static constexpr size_t total = bar_off + K * 8 + 128;  // + alignment slack
     static constexpr uint32_t tx_bytes = 5 * BW * 4 + (STAGE == 2 ? 5 * W * 4 : 0);
 };
 
@@ -93,10 +106,11 @@ template <int NT, int K, int STAGE, int SCHEME, int LIM>
 __global__ void __launch_bounds__(NT) k_stage(const __grid_constant__ CUtensorMap tm_in,
                                               const __grid_constant__ CUtensorMap tm_blend, const StepArgs a) {
     using L = StageLayout<NT, K, STAGE>;
-    constexpr int W = L::W, BW = L::BW, PR = L::PR, XR = L::XR;
+    constexpr int W = L::W, PR = L::PR, XR = L::XR;
     static_assert(L::total <= 227 * 1024, "shared memory");
     constexpr int AHEAD = K - 3;
-    extern __shared__ __align__(128) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char *smem = aligned_smem(smem_raw);
     float *raw = reinterpret_cast<float *>(smem + L::raw_off);
     float *bl = reinterpret_cast<float *>(smem + L::bl_off);
     float4 *P = reinterpret_cast<float4 *>(smem + L::p_off);
@@ -130,8 +144,8 @@ __global__ void __launch_bounds__(NT) k_stage(const __grid_constant__ CUtensorMa
         mbar_arrive_expect_tx(&bars[slot], L::tx_bytes);
 #pragma unroll
         for (int b = 0; b < L::NB; b++)
-            tma_load_3d(raw + (size_t)slot * 5 * BW + b * 5 * kBox, &tm_in, &bars[slot], i0 - 4 + b * kBox, row, 0);
-        if (STAGE == 2) tma_load_3d(bl + (size_t)slot * 5 * W, &tm_blend, &bars[slot], i0, row, 0);
+            tma_load_3d(raw + (size_t)slot * L::SLOT + b * kBoxStride, &tm_in, &bars[slot], i0 - 4 + b * kBox, row, 0);
+        if (STAGE == 2) tma_load_3d(bl + (size_t)slot * L::BSLOT, &tm_blend, &bars[slot], i0, row, 0);
     };
     if (t == 0)
         for (int q = 0; q < min(AHEAD, nrows); q++) issue(q);
@@ -149,7 +163,7 @@ __global__ void __launch_bounds__(NT) k_stage(const __grid_constant__ CUtensorMa
             const int i = i0 - 2 + t;
             const int ic = clampi(i, 0, nx - 1);
             const int rc = ic - i0 + 4;
-            const float *src = raw + (size_t)slot * 5 * BW;
+            const float *src = raw + (size_t)slot * L::SLOT;
             float u, v, p, T;
             const float rho = ring_at<L::NB>(src, 0, rc);
             prim_from_cons(rho, ring_at<L::NB>(src, 1, rc), ring_at<L::NB>(src, 2, rc), ring_at<L::NB>(src, 3, rc),
@@ -206,7 +220,7 @@ __global__ void __launch_bounds__(NT) k_stage(const __grid_constant__ CUtensorMa
             const int su = (urow % PR + PR) % PR;
             const uint32_t mb = M[su * NT + c];
             const int uslot = (q - 2) % K;
-            const float *src = raw + (size_t)uslot * 5 * BW;
+            const float *src = raw + (size_t)uslot * L::SLOT;
             float Uc[5], Un[5];
 #pragma unroll
             for (int k = 0; k < 5; k++) Uc[k] = ring_at<L::NB>(src, k, t + 4);
@@ -235,7 +249,7 @@ __global__ void __launch_bounds__(NT) k_stage(const __grid_constant__ CUtensorMa
                             Un);
             }
             if (STAGE == 2) {
-                const float *b = bl + (size_t)uslot * 5 * W;
+                const float *b = bl + (size_t)uslot * L::BSLOT;
 #pragma unroll
                 for (int k = 0; k < 5; k++) Un[k] = 0.5f * b[k * W + t] + 0.5f * Un[k];
             }
@@ -269,8 +283,9 @@ struct ViscLayout {
     static constexpr int BW = NB * kBox;
     static constexpr int PR = 5;
     static constexpr int TR = 3;
+    static constexpr int SLOT = NB * kBoxStride;
     static constexpr size_t raw_off = 0;
-    static constexpr size_t raw_bytes = (size_t)K * 5 * BW * 4;
+    static constexpr size_t raw_bytes = (size_t)K * SLOT * 4;
     static constexpr size_t p_off = raw_off + raw_bytes;
     static constexpr size_t p_bytes = (size_t)PR * NT * 16;
     static constexpr size_t t_off = p_off + p_bytes;
@@ -278,7 +293,7 @@ struct ViscLayout {
     static constexpr size_t m_off = t_off + t_bytes;
     static constexpr size_t m_bytes = (size_t)PR * NT;
     static constexpr size_t bar_off = (m_off + m_bytes + 15) & ~(size_t)15;
-    static constexpr size_t total = bar_off + K * 8;
+    static constexpr size_t total = bar_off + K * 8 + 128;  // + alignment slack
     static constexpr uint32_t tx_bytes = 5 * BW * 4;
 };
 
@@ -288,9 +303,10 @@ struct ViscLayout {
 template <int NT, int K>
 __global__ void __launch_bounds__(NT) k_viscous(const __grid_constant__ CUtensorMap tm_in, const StepArgs a) {
     using L = ViscLayout<NT, K>;
-    constexpr int W = L::W, BW = L::BW, PR = L::PR, TR = L::TR;
+    constexpr int W = L::W, PR = L::PR, TR = L::TR;
     constexpr int AHEAD = K - 3;
-    extern __shared__ __align__(128) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char *smem = aligned_smem(smem_raw);
     float *raw = reinterpret_cast<float *>(smem + L::raw_off);
     float4 *P = reinterpret_cast<float4 *>(smem + L::p_off);  // {u, v, T, -}
     float *Tq = reinterpret_cast<float *>(smem + L::t_off);   // {txx, tyy, txy, qx, qy}
@@ -327,7 +343,7 @@ __global__ void __launch_bounds__(NT) k_viscous(const __grid_constant__ CUtensor
         mbar_arrive_expect_tx(&bars[slot], L::tx_bytes);
 #pragma unroll
         for (int b = 0; b < L::NB; b++)
-            tma_load_3d(raw + (size_t)slot * 5 * BW + b * 5 * kBox, &tm_in, &bars[slot], i0 - 4 + b * kBox, row, 0);
+            tma_load_3d(raw + (size_t)slot * L::SLOT + b * kBoxStride, &tm_in, &bars[slot], i0 - 4 + b * kBox, row, 0);
     };
     if (t == 0)
         for (int q = 0; q < min(AHEAD, nrows); q++) issue(q);
@@ -344,7 +360,7 @@ __global__ void __launch_bounds__(NT) k_viscous(const __grid_constant__ CUtensor
             const int i = i0 - 2 + t;
             const int ic = clampi(i, 0, nx - 1);
             const int rc = ic - i0 + 4;
-            const float *src = raw + (size_t)slot * 5 * BW;
+            const float *src = raw + (size_t)slot * L::SLOT;
             float u, v, p, T;
             prim_from_cons(ring_at<L::NB>(src, 0, rc), ring_at<L::NB>(src, 1, rc), ring_at<L::NB>(src, 2, rc),
                            ring_at<L::NB>(src, 3, rc), ring_at<L::NB>(src, 4, rc), u, v, p, T);
@@ -392,7 +408,7 @@ __global__ void __launch_bounds__(NT) k_viscous(const __grid_constant__ CUtensor
             const uint32_t mb = M[su * NT + c];
             const uint32_t ctype = mb_type(mb);
             const int uslot = (q - 2) % K;
-            const float *src = raw + (size_t)uslot * 5 * BW;
+            const float *src = raw + (size_t)uslot * L::SLOT;
             float U[5];
 #pragma unroll
             for (int k = 0; k < 5; k++) U[k] = ring_at<L::NB>(src, k, t + 4);
@@ -446,8 +462,6 @@ __global__ void __launch_bounds__(NT) k_viscous(const __grid_constant__ CUtensor
 }
 
 // ------------------------------------------------------------- ghost pass
-__constant__ int c_nbr[8][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}, {-1, -1}, {1, -1}, {-1, 1}, {1, 1}};
-
 __device__ __forceinline__ float pre_bc(const GhostArgs &a, long long q, int k) {
     const long long o = (long long)k * a.g.plane + q;
     return a.B2 ? (0.5f * a.B1[o] + 0.5f * a.B2[o]) : a.B1[o];
@@ -494,7 +508,9 @@ __global__ void __launch_bounds__(128) k_ghost(const GhostArgs a) {
             const int code = (gi.cand >> (4 * m)) & 0xF;
             const int d = code & 7;
             const bool gh = (code & 8) != 0;
-            const long long q = (long long)gi.pidx + c_nbr[d][0] + (long long)c_nbr[d][1] * a.g.pitch;
+            int di, dj;
+            ghost_neighbour(d, di, dj);
+            const long long q = (long long)gi.pidx + di + (long long)dj * a.g.pitch;
             const float rq = gh ? pre_bc(a, q, 0) : a.A[q];
             if (rq >= MIN_DENSITY) {
                 best = q;

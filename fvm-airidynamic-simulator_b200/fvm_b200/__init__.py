@@ -28,7 +28,7 @@ EXPORTS = [
     "fvm_write_fields", "fvm_read_primitives", "fvm_field_to_device", "fvm_cell_types_to_device",
     "fvm_vector_arrows", "fvm_max_temperature", "fvm_max_mach", "fvm_memory_usage", "fvm_gpu_mem_info",
     "fvm_diagnostics", "fvm_shock_standoff", "fvm_set_kernel_timing", "fvm_kernel_times",
-    "fvm_launch_count", "fvm_build_info",
+    "fvm_launch_count", "fvm_debug_stage1", "fvm_debug_ghost_table", "fvm_build_info",
 ]
 
 
@@ -92,6 +92,8 @@ def load_library(path=None):
     lib.fvm_set_kernel_timing.argtypes = [vp, i]
     lib.fvm_kernel_times.argtypes = [vp, C.POINTER(KernelTime), i, C.POINTER(i)]
     lib.fvm_launch_count.argtypes = [vp, C.POINTER(C.c_longlong)]
+    lib.fvm_debug_stage1.argtypes = [vp, f, i] + [vp] * 5
+    lib.fvm_debug_ghost_table.argtypes = [vp, vp, i, C.POINTER(i)]
     _lib = lib
     return lib
 
@@ -251,6 +253,19 @@ class Solver:
         n = C.c_int()
         _check(self.lib.fvm_kernel_times(self.h, arr, cap, C.byref(n)))
         return {arr[k].name.decode(): (arr[k].launches, arr[k].total_ms) for k in range(min(n.value, cap))}
+
+    def debug_stage1(self, dt, with_ghost=True):
+        n = self.params.nx * self.params.ny
+        out = [np.empty(n, np.float32) for _ in range(5)]
+        _check(self.lib.fvm_debug_stage1(self.h, float(dt), 1 if with_ghost else 0, *[_p(x) for x in out]))
+        return np.stack([x.reshape(self.shape) for x in out])
+
+    def debug_ghost_table(self):
+        n = C.c_int()
+        _check(self.lib.fvm_debug_ghost_table(self.h, None, 0, C.byref(n)))
+        out = np.zeros((max(n.value, 1), 7), np.int32)
+        _check(self.lib.fvm_debug_ghost_table(self.h, _p(out), n.value, C.byref(n)))
+        return out[:n.value]
 
     def launch_count(self):
         v = C.c_longlong()

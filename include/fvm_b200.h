@@ -224,6 +224,17 @@ int fvm_kernel_times(fvm_handle *h, fvm_kernel_time *out, int cap, int *count_ou
 /* Count of kernels this library launched on the handle since creation. */
 int fvm_launch_count(fvm_handle *h, long long *count_out);
 
+/* Test hook: run stage 1 of the next step (inviscid stage kernel, and the
+ * ghost-cell pass when with_ghost != 0) from the current state with dt and
+ * copy U* to the five host arrays (nx*ny each).  The state is not advanced. */
+int fvm_debug_stage1(fvm_handle *h, float dt, int with_ghost, float *rho, float *rho_u, float *rho_v, float *E,
+                     float *rho_e);
+
+/* Test hook: copy the ghost-cell table (7 ints per ghost cell: pitched index,
+ * i, j, normal x and y as float bits, packed candidate codes, count) to
+ * `out` (cap entries); *count_out receives the number of ghost cells. */
+int fvm_debug_ghost_table(fvm_handle *h, int *out, int cap, int *count_out);
+
 /* Library build description (arch, flags). */
 const char *fvm_build_info(void);
 

@@ -53,7 +53,7 @@ def _lib(bits):
     lib.orc_get_primitives.argtypes = [vp] + [C.c_void_p] * 4
     lib.orc_get_mu.argtypes = [vp, C.c_void_p]
     lib.orc_get_geometry.argtypes = [vp, C.c_void_p, C.c_void_p]
-    lib.orc_stage1.argtypes = [vp, d, C.c_void_p * 5]
+    lib.orc_stage1.argtypes = [vp, d, i, C.c_void_p * 5]
     lib.orc_diagnostics.argtypes = [vp, C.POINTER(Diag)]
     lib.orc_shock_standoff.argtypes = [vp]
     lib.orc_shock_standoff.restype = d
@@ -148,10 +148,10 @@ class Oracle:
         self.lib.orc_get_geometry(self.h, _ptr(sdf), _ptr(ct))
         return sdf.reshape(self.shape), ct.reshape(self.shape)
 
-    def stage1(self, dt):
+    def stage1(self, dt, with_ghost=True):
         out = [np.empty(self.nx * self.ny, np.float64) for _ in range(5)]
         arr = (C.c_void_p * 5)(*[a.ctypes.data for a in out])
-        self.lib.orc_stage1(self.h, float(dt), arr)
+        self.lib.orc_stage1(self.h, float(dt), 1 if with_ghost else 0, arr)
         return np.stack([a.reshape(self.shape) for a in out])
 
     def diagnostics(self):

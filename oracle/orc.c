@@ -1085,10 +1085,16 @@ void orc_step(orc_solver *s, double dt_in) {
     primitives(s, s->U);
 }
 
-void orc_stage1(orc_solver *s, double dt, double *out5[5]) {
+void orc_stage1(orc_solver *s, double dt, int with_ghost, double *out5[5]) {
     fluxes(s, s->U);
     update(s, s->U, s->Us, (R)dt);
-    apply_bc(s, s->Us);
+    if (with_ghost) {
+        apply_bc(s, s->Us);
+    } else {
+        const int nx = s->nx, ny = s->ny;
+        for (int j = 0; j < ny; j++)
+            for (int i = 0; i < nx; i++) bc_pointwise(s, s->Us, i, j);
+    }
     for (int k = 0; k < 5; k++)
         if (out5[k])
             for (size_t c = 0; c < s->n; c++) out5[k][c] = (double)s->Us[k][c];

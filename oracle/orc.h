@@ -71,7 +71,7 @@ void orc_get_mu(orc_solver *s, double *mu);
 void orc_get_geometry(orc_solver *s, double *sdf, uint8_t *ct);
 
 /* Stage-level entry points (for localising differences). */
-void orc_stage1(orc_solver *s, double dt, double *out5[5]);
+void orc_stage1(orc_solver *s, double dt, int with_ghost, double *out5[5]);
 
 /* Diagnostics with the same definitions as the device reductions. */
 void orc_diagnostics(orc_solver *s, fvm_diag *out);

@@ -72,6 +72,13 @@ void ref_write_fields(void *h, const float *rho, const float *ru, const float *r
     cudaMemcpy(s->d_rho_v_, rv, n, cudaMemcpyHostToDevice);
     cudaMemcpy(s->d_E_, E, n, cudaMemcpyHostToDevice);
     cudaMemcpy(s->d_rho_e_, re, n, cudaMemcpyHostToDevice);
+    // step() expects the primitives (and mu) of the current state, as left
+    // by reset or by the previous step (src/solver.cu:3291-3293, :3148-3158)
+    s->launchComputePrimitivesKernel(s->d_rho_, s->d_rho_u_, s->d_rho_v_, s->d_E_, s->d_rho_e_, s->d_u_, s->d_v_,
+                                     s->d_p_, s->d_T_, s->_nx, s->_ny);
+    s->launchFusedViscousDiffusionKernel(s->d_u_, s->d_v_, s->d_T_, s->d_mu_, s->d_rho_u_, s->d_rho_v_, s->d_E_,
+                                         s->d_rho_e_, s->d_cell_type_, 0.0f, 1.0f, 1.0f, s->_nx, s->_ny);
+    cudaDeviceSynchronize();
 }
 
 void ref_read_primitives(void *h, float *u, float *v, float *p, float *T) {

@@ -124,43 +124,36 @@ __device__ __forceinline__ void hllc_flux(float rhoL, float unL, float utL, floa
     float denom_star = rhoL * (SL - unL) - rhoR * (SR - unR);
     float safe_denom_star = copysignf(fmaxf(fabsf(denom_star), 1e-10f), denom_star);
     float S_star = (pR - pL + rhoL * unL * (SL - unL) - rhoR * unR * (SR - unR)) / safe_denom_star;
-    if (SL >= 0.0f) {
-        phys_flux<XDIR>(rhoL, unL, utL, pL, EL, f);
-    } else if (SR <= 0.0f) {
-        phys_flux<XDIR>(rhoR, unR, utR, pR, ER, f);
-    } else if (S_star >= 0.0f) {
-        float coeff_denom = SL - S_star;
-        if (fabsf(coeff_denom) < 1e-10f) coeff_denom = (coeff_denom >= 0) ? 1e-10f : -1e-10f;
-        float rho_star = rhoL * (SL - unL) / coeff_denom;
-        rho_star = fmaxf(rho_star, MIN_DENSITY);
-        float mn_star = rho_star * S_star;
-        float mt_star = rho_star * utL;
-        float p_star = pL + rhoL * (SL - unL) * (S_star - unL);
-        p_star = fmaxf(p_star, MIN_PRESSURE);
-        float E_star = (EL * (SL - unL) + p_star * S_star - pL * unL) / coeff_denom;
-        float fl[4];
-        phys_flux<XDIR>(rhoL, unL, utL, pL, EL, fl);
-        f[0] = fl[0] + SL * (rho_star - rhoL);
-        f[1] = fl[1] + SL * (mn_star - rhoL * unL);
-        f[2] = fl[2] + SL * (mt_star - rhoL * utL);
-        f[3] = fl[3] + SL * (E_star - EL);
-    } else {
-        float coeff_denom = SR - S_star;
-        if (fabsf(coeff_denom) < 1e-10f) coeff_denom = (coeff_denom >= 0) ? 1e-10f : -1e-10f;
-        float coeff = rhoR * (SR - unR) / coeff_denom;
-        coeff = fmaxf(coeff, MIN_DENSITY);
-        float mn_star = coeff * S_star;
-        float mt_star = coeff * utR;
-        float p_star = pR + rhoR * (SR - unR) * (S_star - unR);
-        p_star = fmaxf(p_star, MIN_PRESSURE);
-        float E_star = (ER * (SR - unR) + p_star * S_star - pR * unR) / coeff_denom;
-        float fr[4];
-        phys_flux<XDIR>(rhoR, unR, utR, pR, ER, fr);
-        f[0] = fr[0] + SR * (coeff - rhoR);
-        f[1] = fr[1] + SR * (mn_star - rhoR * unR);
-        f[2] = fr[2] + SR * (mt_star - rhoR * utR);
-        f[3] = fr[3] + SR * (E_star - ER);
-    }
+    // Upwind side K of the wave fan: L if all waves move right (SL >= 0) or
+    // the contact does (S* >= 0), R otherwise.  The reference branches four
+    // ways (src/solver.cu:1160-1222); selecting K's operands and evaluating
+    // the shared star-state expressions once gives the same value per face
+    // without divergence.
+    const bool supL = SL >= 0.0f;
+    const bool supR = !supL && SR <= 0.0f;
+    const bool useL = supL || (!supR && S_star >= 0.0f);
+    const float rK = useL ? rhoL : rhoR;
+    const float unK = useL ? unL : unR;
+    const float utK = useL ? utL : utR;
+    const float pK = useL ? pL : pR;
+    const float EK = useL ? EL : ER;
+    const float SK = useL ? SL : SR;
+    float fK[4];
+    phys_flux<XDIR>(rK, unK, utK, pK, EK, fK);
+    float coeff_denom = SK - S_star;
+    if (fabsf(coeff_denom) < 1e-10f) coeff_denom = (coeff_denom >= 0) ? 1e-10f : -1e-10f;
+    float rho_star = rK * (SK - unK) / coeff_denom;
+    rho_star = fmaxf(rho_star, MIN_DENSITY);
+    float mn_star = rho_star * S_star;
+    float mt_star = rho_star * utK;
+    float p_star = pK + rK * (SK - unK) * (S_star - unK);
+    p_star = fmaxf(p_star, MIN_PRESSURE);
+    float E_star = (EK * (SK - unK) + p_star * S_star - pK * unK) / coeff_denom;
+    const bool star = !(supL || supR);
+    f[0] = star ? fK[0] + SK * (rho_star - rK) : fK[0];
+    f[1] = star ? fK[1] + SK * (mn_star - rK * unK) : fK[1];
+    f[2] = star ? fK[2] + SK * (mt_star - rK * utK) : fK[2];
+    f[3] = star ? fK[3] + SK * (E_star - EK) : fK[3];
 }
 
 // AUSM+ (Liou 1996, J. Comput. Phys. 129:364-382); no reference counterpart.

@@ -153,57 +153,67 @@ __global__ void __launch_bounds__(NT) k_stage(const __grid_constant__ CUtensorMa
     float lmax_speed = 0.0f;
     int issued = min(AHEAD, nrows);
     bool aborted = false;
+    // mask bytes of this thread's column, prefetched two rows ahead
+    const int ic_t = clampi(i0 - 2 + t, 0, nx - 1);
+    const uint8_t *mcol = a.mask + ic_t;
+    uint32_t m_cur = __ldg(mcol + (size_t)clampi(rs, 0, ny - 1) * g.pitch);
+    uint32_t m_nxt = __ldg(mcol + (size_t)clampi(rs + 1, 0, ny - 1) * g.pitch);
 
     for (int q = 0; q < nrows; q++) {
         const int r = rs + q;
         const int slot = q % K;
+        const uint32_t m_pf = __ldg(mcol + (size_t)clampi(r + 2, 0, ny - 1) * g.pitch);
         // ---- phase 1: primitives + mask of the incoming row
         bool ok = mbar_wait_bounded(&bars[slot], (uint32_t)((q / K) & 1));
         if (ok) {
-            const int i = i0 - 2 + t;
-            const int ic = clampi(i, 0, nx - 1);
-            const int rc = ic - i0 + 4;
+            const int rc = ic_t - i0 + 4;
             const float *src = raw + (size_t)slot * L::SLOT;
             float u, v, p, T;
             const float rho = ring_at<L::NB>(src, 0, rc);
             prim_from_cons(rho, ring_at<L::NB>(src, 1, rc), ring_at<L::NB>(src, 2, rc), ring_at<L::NB>(src, 3, rc),
                            ring_at<L::NB>(src, 4, rc), u, v, p, T);
             P[(r % PR + PR) % PR * NT + t] = make_float4(rho, u, v, p);
-            M[(r % PR + PR) % PR * NT + t] = a.mask[(size_t)clampi(r, 0, ny - 1) * g.pitch + ic];
+            M[(r % PR + PR) % PR * NT + t] = (uint8_t)m_cur;
         }
+        m_cur = m_nxt;
+        m_nxt = m_pf;
         if (__syncthreads_or(!ok)) {
             aborted = true;
             break;
         }
         const int sr = (r % PR + PR) % PR;
-        // ---- phase 2a: x-faces of row r (face of cell i0-1+t, t in [0, W])
-        if (r >= j0 && t <= W) {
+        // ---- phase 2: x-face of row r owned by cell i0-1+t (t in [0, W]) and
+        // the y-face between rows r-2 and r-1 at column i0+t (t < W).  Both are
+        // evaluated by every thread (operands clamped in range) so the two
+        // independent Riemann problems interleave; only needed ones are stored.
+        {
+            const int tx = min(t, W);
             const float4 *Pr = P + sr * NT;
-            const uint32_t mb = M[sr * NT + t + 1];
-            const float4 m1 = Pr[t], aa = Pr[t + 1], bb = Pr[t + 2], p2 = Pr[t + 3];
-            float f[5];
-            face_flux<true, SCHEME, LIM>((mb & MB_XV) != 0, (mb & MB_XN) != 0, Prim{m1.x, m1.y, m1.z, m1.w},
-                                         Prim{aa.x, aa.y, aa.z, aa.w}, Prim{bb.x, bb.y, bb.z, bb.w},
-                                         Prim{p2.x, p2.y, p2.z, p2.w}, f);
-            float *Xs = X + (size_t)((r % XR + XR) % XR) * 5 * NT;
+            const uint32_t mbx = M[sr * NT + tx + 1];
+            const float4 xm1 = Pr[tx], xa = Pr[tx + 1], xb = Pr[tx + 2], xp2 = Pr[tx + 3];
+            const int c = min(t, W - 1) + 2;
+            const float4 ym1 = P[((r - 3) % PR + PR) % PR * NT + c];
+            const float4 ya = P[((r - 2) % PR + PR) % PR * NT + c];
+            const float4 yb = P[((r - 1) % PR + PR) % PR * NT + c];
+            const float4 yp2 = P[sr * NT + c];
+            const uint32_t mby = M[((r - 2) % PR + PR) % PR * NT + c];
+            float fx[5], fy[5];
+            face_flux<true, SCHEME, LIM>((mbx & MB_XV) != 0, (mbx & MB_XN) != 0, Prim{xm1.x, xm1.y, xm1.z, xm1.w},
+                                         Prim{xa.x, xa.y, xa.z, xa.w}, Prim{xb.x, xb.y, xb.z, xb.w},
+                                         Prim{xp2.x, xp2.y, xp2.z, xp2.w}, fx);
+            face_flux<false, SCHEME, LIM>((mby & MB_YV) != 0, (mby & MB_YN) != 0, Prim{ym1.x, ym1.y, ym1.z, ym1.w},
+                                          Prim{ya.x, ya.y, ya.z, ya.w}, Prim{yb.x, yb.y, yb.z, yb.w},
+                                          Prim{yp2.x, yp2.y, yp2.z, yp2.w}, fy);
+            if (r >= j0 && t <= W) {
+                float *Xs = X + (size_t)((r % XR + XR) % XR) * 5 * NT;
 #pragma unroll
-            for (int k = 0; k < 5; k++) Xs[k * NT + t] = f[k];
-        }
-        // ---- phase 2b: y-face between rows r-2 and r-1 at column i0+t
-        if (r >= j0 + 1 && t < W) {
-            const int c = t + 2;
-            const float4 m1 = P[((r - 3) % PR + PR) % PR * NT + c];
-            const float4 aa = P[((r - 2) % PR + PR) % PR * NT + c];
-            const float4 bb = P[((r - 1) % PR + PR) % PR * NT + c];
-            const float4 p2 = P[sr * NT + c];
-            const uint32_t mb = M[((r - 2) % PR + PR) % PR * NT + c];
-            float f[5];
-            face_flux<false, SCHEME, LIM>((mb & MB_YV) != 0, (mb & MB_YN) != 0, Prim{m1.x, m1.y, m1.z, m1.w},
-                                          Prim{aa.x, aa.y, aa.z, aa.w}, Prim{bb.x, bb.y, bb.z, bb.w},
-                                          Prim{p2.x, p2.y, p2.z, p2.w}, f);
-            float *Ys = Y + (size_t)((r - 2) & 1) * 5 * NT;
+                for (int k = 0; k < 5; k++) Xs[k * NT + t] = fx[k];
+            }
+            if (r >= j0 + 1 && t < W) {
+                float *Ys = Y + (size_t)((r - 2) & 1) * 5 * NT;
 #pragma unroll
-            for (int k = 0; k < 5; k++) Ys[k * NT + t] = f[k];
+                for (int k = 0; k < 5; k++) Ys[k * NT + t] = fy[k];
+            }
         }
         fence_proxy_async_smem();
         __syncthreads();
@@ -350,23 +360,28 @@ __global__ void __launch_bounds__(NT) k_viscous(const __grid_constant__ CUtensor
     int issued = min(AHEAD, nrows);
     bool aborted = false;
     float lmax_speed = 0.0f, lmax_nu = 0.0f;
+    const int ic_t = clampi(i0 - 2 + t, 0, nx - 1);
+    const uint8_t *mcol = a.mask + ic_t;
+    uint32_t m_cur = __ldg(mcol + (size_t)clampi(rs, 0, ny - 1) * g.pitch);
+    uint32_t m_nxt = __ldg(mcol + (size_t)clampi(rs + 1, 0, ny - 1) * g.pitch);
 
     for (int q = 0; q < nrows; q++) {
         const int r = rs + q;
         const int slot = q % K;
         const int sr = (r % PR + PR) % PR;
+        const uint32_t m_pf = __ldg(mcol + (size_t)clampi(r + 2, 0, ny - 1) * g.pitch);
         bool ok = mbar_wait_bounded(&bars[slot], (uint32_t)((q / K) & 1));
         if (ok) {
-            const int i = i0 - 2 + t;
-            const int ic = clampi(i, 0, nx - 1);
-            const int rc = ic - i0 + 4;
+            const int rc = ic_t - i0 + 4;
             const float *src = raw + (size_t)slot * L::SLOT;
             float u, v, p, T;
             prim_from_cons(ring_at<L::NB>(src, 0, rc), ring_at<L::NB>(src, 1, rc), ring_at<L::NB>(src, 2, rc),
                            ring_at<L::NB>(src, 3, rc), ring_at<L::NB>(src, 4, rc), u, v, p, T);
             P[sr * NT + t] = make_float4(u, v, T, 0.0f);
-            M[sr * NT + t] = a.mask[(size_t)clampi(r, 0, ny - 1) * g.pitch + ic];
+            M[sr * NT + t] = (uint8_t)m_cur;
         }
+        m_cur = m_nxt;
+        m_nxt = m_pf;
         if (__syncthreads_or(!ok)) {
             aborted = true;
             break;

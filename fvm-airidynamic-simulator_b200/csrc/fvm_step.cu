@@ -100,6 +100,13 @@ struct StageLayout {
     static constexpr uint32_t tx_bytes = 5 * BW * 4 + (STAGE == 2 ? 5 * W * 4 : 0);
 };
 
+// Slot bookkeeping of a row ring of N slots: rotating the indices of the
+// last few rows avoids integer division in the row loop.
+template <int N>
+__device__ __forceinline__ int ring_next(int s) {
+    return (s + 1 == N) ? 0 : s + 1;
+}
+
 // Inviscid SSP-RK2 stage (computeFluxesKernel + updateKernel + [blend] +
 // phase-1 BC, src/solver.cu:1450-1876, :949-967, :1891-2042).
 template <int NT, int K, int STAGE, int SCHEME, int LIM>
@@ -108,6 +115,7 @@ __global__ void __launch_bounds__(NT) k_stage(const __grid_constant__ CUtensorMa
     using L = StageLayout<NT, K, STAGE>;
     constexpr int W = L::W, PR = L::PR, XR = L::XR;
     static_assert(L::total <= 227 * 1024, "shared memory");
+    static_assert(PR == 5 && XR == 3, "ring sizes");
     constexpr int AHEAD = K - 3;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     unsigned char *smem = aligned_smem(smem_raw);
@@ -155,25 +163,37 @@ __global__ void __launch_bounds__(NT) k_stage(const __grid_constant__ CUtensorMa
     bool aborted = false;
     // mask bytes of this thread's column, prefetched two rows ahead
     const int ic_t = clampi(i0 - 2 + t, 0, nx - 1);
+    const int rc_t = ic_t - i0 + 4;
     const uint8_t *mcol = a.mask + ic_t;
     uint32_t m_cur = __ldg(mcol + (size_t)clampi(rs, 0, ny - 1) * g.pitch);
     uint32_t m_nxt = __ldg(mcol + (size_t)clampi(rs + 1, 0, ny - 1) * g.pitch);
+    // per-thread constants of the update phase
+    const int iu = i0 + t;                  // update column
+    const bool col_ok = (t < W) && (iu < nx);
+    const bool edge_x = (iu == 0 || iu == nx - 1);
+    const int tx = min(t, W);               // x-face owner column (clamped)
+    const int cy = min(t, W - 1) + 2;       // y-face / update column in the staged row
+    float *outp = a.out + iu;
+
+    // rotating ring slots: raw (K) of rows r and r-2, parity of row r;
+    // primitive/mask ring (5) of rows r .. r-4; x-face ring (3) of rows r, r-2
+    int kr = 0, ku = K - 2, par = 0;
+    int p0 = 0, p1 = PR - 1, p2 = PR - 2, p3 = PR - 3;
+    int x0 = 0, x2 = XR - 2;
 
     for (int q = 0; q < nrows; q++) {
         const int r = rs + q;
-        const int slot = q % K;
         const uint32_t m_pf = __ldg(mcol + (size_t)clampi(r + 2, 0, ny - 1) * g.pitch);
         // ---- phase 1: primitives + mask of the incoming row
-        bool ok = mbar_wait_bounded(&bars[slot], (uint32_t)((q / K) & 1));
+        bool ok = mbar_wait_bounded(&bars[kr], (uint32_t)par);
         if (ok) {
-            const int rc = ic_t - i0 + 4;
-            const float *src = raw + (size_t)slot * L::SLOT;
+            const float *src = raw + (size_t)kr * L::SLOT;
             float u, v, p, T;
-            const float rho = ring_at<L::NB>(src, 0, rc);
-            prim_from_cons(rho, ring_at<L::NB>(src, 1, rc), ring_at<L::NB>(src, 2, rc), ring_at<L::NB>(src, 3, rc),
-                           ring_at<L::NB>(src, 4, rc), u, v, p, T);
-            P[(r % PR + PR) % PR * NT + t] = make_float4(rho, u, v, p);
-            M[(r % PR + PR) % PR * NT + t] = (uint8_t)m_cur;
+            const float rho = ring_at<L::NB>(src, 0, rc_t);
+            prim_from_cons(rho, ring_at<L::NB>(src, 1, rc_t), ring_at<L::NB>(src, 2, rc_t),
+                           ring_at<L::NB>(src, 3, rc_t), ring_at<L::NB>(src, 4, rc_t), u, v, p, T);
+            P[p0 * NT + t] = make_float4(rho, u, v, p);
+            M[p0 * NT + t] = (uint8_t)m_cur;
         }
         m_cur = m_nxt;
         m_nxt = m_pf;
@@ -181,22 +201,19 @@ __global__ void __launch_bounds__(NT) k_stage(const __grid_constant__ CUtensorMa
             aborted = true;
             break;
         }
-        const int sr = (r % PR + PR) % PR;
         // ---- phase 2: x-face of row r owned by cell i0-1+t (t in [0, W]) and
         // the y-face between rows r-2 and r-1 at column i0+t (t < W).  Both are
         // evaluated by every thread (operands clamped in range) so the two
         // independent Riemann problems interleave; only needed ones are stored.
         {
-            const int tx = min(t, W);
-            const float4 *Pr = P + sr * NT;
-            const uint32_t mbx = M[sr * NT + tx + 1];
+            const float4 *Pr = P + p0 * NT;
+            const uint32_t mbx = M[p0 * NT + tx + 1];
             const float4 xm1 = Pr[tx], xa = Pr[tx + 1], xb = Pr[tx + 2], xp2 = Pr[tx + 3];
-            const int c = min(t, W - 1) + 2;
-            const float4 ym1 = P[((r - 3) % PR + PR) % PR * NT + c];
-            const float4 ya = P[((r - 2) % PR + PR) % PR * NT + c];
-            const float4 yb = P[((r - 1) % PR + PR) % PR * NT + c];
-            const float4 yp2 = P[sr * NT + c];
-            const uint32_t mby = M[((r - 2) % PR + PR) % PR * NT + c];
+            const float4 ym1 = P[p3 * NT + cy];
+            const float4 ya = P[p2 * NT + cy];
+            const float4 yb = P[p1 * NT + cy];
+            const float4 yp2 = Pr[cy];
+            const uint32_t mby = M[p2 * NT + cy];
             float fx[5], fy[5];
             face_flux<true, SCHEME, LIM>((mbx & MB_XV) != 0, (mbx & MB_XN) != 0, Prim{xm1.x, xm1.y, xm1.z, xm1.w},
                                          Prim{xa.x, xa.y, xa.z, xa.w}, Prim{xb.x, xb.y, xb.z, xb.w},
@@ -205,14 +222,14 @@ __global__ void __launch_bounds__(NT) k_stage(const __grid_constant__ CUtensorMa
                                           Prim{ya.x, ya.y, ya.z, ya.w}, Prim{yb.x, yb.y, yb.z, yb.w},
                                           Prim{yp2.x, yp2.y, yp2.z, yp2.w}, fy);
             if (r >= j0 && t <= W) {
-                float *Xs = X + (size_t)((r % XR + XR) % XR) * 5 * NT;
+                float *Xs = X + x0 * 5 * NT + t;
 #pragma unroll
-                for (int k = 0; k < 5; k++) Xs[k * NT + t] = fx[k];
+                for (int k = 0; k < 5; k++) Xs[k * NT] = fx[k];
             }
             if (r >= j0 + 1 && t < W) {
-                float *Ys = Y + (size_t)((r - 2) & 1) * 5 * NT;
+                float *Ys = Y + ((r - 2) & 1) * 5 * NT + t;
 #pragma unroll
-                for (int k = 0; k < 5; k++) Ys[k * NT + t] = fy[k];
+                for (int k = 0; k < 5; k++) Ys[k * NT] = fy[k];
             }
         }
         fence_proxy_async_smem();
@@ -224,13 +241,9 @@ __global__ void __launch_bounds__(NT) k_stage(const __grid_constant__ CUtensorMa
         }
         // ---- phase 3: update row r-2
         const int urow = r - 2;
-        const int i = i0 + t;
-        if (urow >= j0 && urow < j1 && t < W && i < nx) {
-            const int c = t + 2;
-            const int su = (urow % PR + PR) % PR;
-            const uint32_t mb = M[su * NT + c];
-            const int uslot = (q - 2) % K;
-            const float *src = raw + (size_t)uslot * L::SLOT;
+        if (urow >= j0 && urow < j1 && col_ok) {
+            const uint32_t mb = M[p2 * NT + cy];
+            const float *src = raw + (size_t)ku * L::SLOT;
             float Uc[5], Un[5];
 #pragma unroll
             for (int k = 0; k < 5; k++) Uc[k] = ring_at<L::NB>(src, k, t + 4);
@@ -238,42 +251,51 @@ __global__ void __launch_bounds__(NT) k_stage(const __grid_constant__ CUtensorMa
 #pragma unroll
                 for (int k = 0; k < 5; k++) Un[k] = Uc[k];
             } else {
-                const float *Xs = X + (size_t)((urow % XR + XR) % XR) * 5 * NT;
-                const float *Yt = Y + (size_t)(urow & 1) * 5 * NT;
-                const float *Yb = Y + (size_t)((urow - 1) & 1) * 5 * NT;
+                const float *Xs = X + x2 * 5 * NT + t;
+                const float *Yt = Y + (urow & 1) * 5 * NT + t;
+                const float *Yb = Y + ((urow - 1) & 1) * 5 * NT + t;
                 float fR[5], fL[5], fT[5], fB[5];
 #pragma unroll
                 for (int k = 0; k < 5; k++) {
-                    fR[k] = Xs[k * NT + t + 1];
-                    fL[k] = Xs[k * NT + t];
-                    fT[k] = Yt[k * NT + t];
-                    fB[k] = Yb[k * NT + t];
+                    fR[k] = Xs[k * NT + 1];
+                    fL[k] = Xs[k * NT];
+                    fT[k] = Yt[k * NT];
+                    fB[k] = Yb[k * NT];
                 }
-                const float4 pc = P[su * NT + c];
-                const float rxR = P[su * NT + c + 1].x, rxL = P[su * NT + c - 1].x;
-                const float ryT = P[((urow + 1) % PR + PR) % PR * NT + c].x;
-                const float ryB = P[((urow - 1) % PR + PR) % PR * NT + c].x;
-                const bool edge_x = (i == 0 || i == nx - 1);
+                const float4 pc = P[p2 * NT + cy];
+                const float rxR = P[p2 * NT + cy + 1].x, rxL = P[p2 * NT + cy - 1].x;
+                const float ryT = P[p1 * NT + cy].x;
+                const float ryB = P[p3 * NT + cy].x;
                 const bool edge_y = (urow == 0 || urow == ny - 1);
                 update_cell(Uc, fR, fL, fT, fB, rxR, rxL, ryT, ryB, pc.w, edge_x, edge_y, !edge_x && !edge_y, ua,
                             Un);
             }
             if (STAGE == 2) {
-                const float *b = bl + (size_t)uslot * L::BSLOT;
+                const float *b = bl + (size_t)ku * L::BSLOT + t;
 #pragma unroll
-                for (int k = 0; k < 5; k++) Un[k] = 0.5f * b[k * W + t] + 0.5f * Un[k];
+                for (int k = 0; k < 5; k++) Un[k] = 0.5f * b[k * W] + 0.5f * Un[k];
             }
             const uint32_t ctype = mb_type(mb);
-            if (a.apply_bc) bc_pointwise(Un, ctype, i, urow, nx, ny, a.fs);
+            if (a.apply_bc) bc_pointwise(Un, ctype, iu, urow, nx, ny, a.fs);
             if (a.cfl && ctype != CT_GHOST) {
                 float uu, vv, pp, TT;
                 prim_from_cons(Un[0], Un[1], Un[2], Un[3], Un[4], uu, vv, pp, TT);
                 lmax_speed = fmaxf(lmax_speed, wave_speed(uu, vv, pp, Un[0]));
             }
-            float *dst = a.out + (size_t)urow * g.pitch + i;
+            float *dst = outp + (size_t)urow * g.pitch;
 #pragma unroll
             for (int k = 0; k < 5; k++) dst[k * g.plane] = Un[k];
         }
+        // rotate ring slots to the next row
+        kr = ring_next<K>(kr);
+        par ^= (kr == 0) ? 1 : 0;
+        ku = ring_next<K>(ku);
+        p3 = p2;
+        p2 = p1;
+        p1 = p0;
+        p0 = ring_next<PR>(p0);
+        x0 = ring_next<XR>(x0);
+        x2 = ring_next<XR>(x2);
     }
     if (aborted) {
         if (t == 0) {
@@ -314,6 +336,7 @@ template <int NT, int K>
 __global__ void __launch_bounds__(NT) k_viscous(const __grid_constant__ CUtensorMap tm_in, const StepArgs a) {
     using L = ViscLayout<NT, K>;
     constexpr int W = L::W, PR = L::PR, TR = L::TR;
+    static_assert(PR == 5 && TR == 3, "ring sizes");
     constexpr int AHEAD = K - 3;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     unsigned char *smem = aligned_smem(smem_raw);
@@ -361,24 +384,35 @@ __global__ void __launch_bounds__(NT) k_viscous(const __grid_constant__ CUtensor
     bool aborted = false;
     float lmax_speed = 0.0f, lmax_nu = 0.0f;
     const int ic_t = clampi(i0 - 2 + t, 0, nx - 1);
+    const int rc_t = ic_t - i0 + 4;
     const uint8_t *mcol = a.mask + ic_t;
     uint32_t m_cur = __ldg(mcol + (size_t)clampi(rs, 0, ny - 1) * g.pitch);
     uint32_t m_nxt = __ldg(mcol + (size_t)clampi(rs + 1, 0, ny - 1) * g.pitch);
+    // stress column i0-1+t (t < NT-2) and update column i0+t (t < W)
+    const int is = i0 - 1 + t;
+    const bool stress_col_in = (t < NT - 2) && is >= 0 && is < nx;
+    const int iu = i0 + t;
+    const bool col_ok = (t < W) && (iu < nx);
+    const bool interior_x = iu > 0 && iu < nx - 1;
+    float *outp = a.out + iu;
+
+    // rotating slots: raw ring (K) rows r, r-2; primitives (5) rows r..r-3;
+    // stress ring (3) rows r-1 (written), r-2, r-3
+    int kr = 0, ku = K - 2, par = 0;
+    int p0 = 0, p1 = PR - 1, p2 = PR - 2, p3 = PR - 3;
+    int s1 = 0, s2 = TR - 1, s3 = TR - 2;
 
     for (int q = 0; q < nrows; q++) {
         const int r = rs + q;
-        const int slot = q % K;
-        const int sr = (r % PR + PR) % PR;
         const uint32_t m_pf = __ldg(mcol + (size_t)clampi(r + 2, 0, ny - 1) * g.pitch);
-        bool ok = mbar_wait_bounded(&bars[slot], (uint32_t)((q / K) & 1));
+        bool ok = mbar_wait_bounded(&bars[kr], (uint32_t)par);
         if (ok) {
-            const int rc = ic_t - i0 + 4;
-            const float *src = raw + (size_t)slot * L::SLOT;
+            const float *src = raw + (size_t)kr * L::SLOT;
             float u, v, p, T;
-            prim_from_cons(ring_at<L::NB>(src, 0, rc), ring_at<L::NB>(src, 1, rc), ring_at<L::NB>(src, 2, rc),
-                           ring_at<L::NB>(src, 3, rc), ring_at<L::NB>(src, 4, rc), u, v, p, T);
-            P[sr * NT + t] = make_float4(u, v, T, 0.0f);
-            M[sr * NT + t] = (uint8_t)m_cur;
+            prim_from_cons(ring_at<L::NB>(src, 0, rc_t), ring_at<L::NB>(src, 1, rc_t), ring_at<L::NB>(src, 2, rc_t),
+                           ring_at<L::NB>(src, 3, rc_t), ring_at<L::NB>(src, 4, rc_t), u, v, p, T);
+            P[p0 * NT + t] = make_float4(u, v, T, 0.0f);
+            M[p0 * NT + t] = (uint8_t)m_cur;
         }
         m_cur = m_nxt;
         m_nxt = m_pf;
@@ -389,23 +423,21 @@ __global__ void __launch_bounds__(NT) k_viscous(const __grid_constant__ CUtensor
         // ---- phase 2: stress and heat flux of row r-1 at column i0-1+t
         const int trow = r - 1;
         if (trow >= j0 - 1 && t < NT - 2) {
-            const int i = i0 - 1 + t;
             const int c = t + 1;
-            const int s0 = ((trow) % PR + PR) % PR, sN = sr, sS = ((trow - 1) % PR + PR) % PR;
             float out[5];
-            const uint32_t ct = mb_type(M[s0 * NT + c]);
-            if (i < 0 || i >= nx || trow < 0 || trow >= ny || ct == CT_SOLID) {
+            const uint32_t ct = mb_type(M[p1 * NT + c]);
+            if (!stress_col_in || trow < 0 || trow >= ny || ct == CT_SOLID) {
 #pragma unroll
                 for (int k = 0; k < 5; k++) out[k] = 0.0f;
             } else {
-                const float4 C = P[s0 * NT + c], E = P[s0 * NT + c + 1], Wc = P[s0 * NT + c - 1];
-                const float4 N = P[sN * NT + c], S = P[sS * NT + c];
-                stress_heat(C.x, C.y, C.z, E.x, Wc.x, N.x, S.x, E.y, Wc.y, N.y, S.y, E.z, Wc.z, N.z, S.z, i == 0,
-                            i == nx - 1, trow == 0, trow == ny - 1, va, out);
+                const float4 C = P[p1 * NT + c], E = P[p1 * NT + c + 1], Wc = P[p1 * NT + c - 1];
+                const float4 N = P[p0 * NT + c], S = P[p2 * NT + c];
+                stress_heat(C.x, C.y, C.z, E.x, Wc.x, N.x, S.x, E.y, Wc.y, N.y, S.y, E.z, Wc.z, N.z, S.z, is == 0,
+                            is == nx - 1, trow == 0, trow == ny - 1, va, out);
             }
-            float *Ts = Tq + (size_t)((trow % TR + TR) % TR) * 5 * NT;
+            float *Ts = Tq + s1 * 5 * NT + t;
 #pragma unroll
-            for (int k = 0; k < 5; k++) Ts[k * NT + t] = out[k];
+            for (int k = 0; k < 5; k++) Ts[k * NT] = out[k];
         }
         fence_proxy_async_smem();
         __syncthreads();
@@ -415,35 +447,32 @@ __global__ void __launch_bounds__(NT) k_viscous(const __grid_constant__ CUtensor
         }
         // ---- phase 3: viscous update of row r-2 at column i0+t
         const int urow = r - 2;
-        const int i = i0 + t;
-        if (urow >= j0 && urow < j1 && t < W && i < nx) {
+        if (urow >= j0 && urow < j1 && col_ok) {
             const int c = t + 2;  // primitive column
             const int tc = t + 1; // stress column
-            const int su = (urow % PR + PR) % PR;
-            const uint32_t mb = M[su * NT + c];
+            const uint32_t mb = M[p2 * NT + c];
             const uint32_t ctype = mb_type(mb);
-            const int uslot = (q - 2) % K;
-            const float *src = raw + (size_t)uslot * L::SLOT;
+            const float *src = raw + (size_t)ku * L::SLOT;
             float U[5];
 #pragma unroll
             for (int k = 0; k < 5; k++) U[k] = ring_at<L::NB>(src, k, t + 4);
-            const float4 pc = P[su * NT + c];
-            if (ctype == CT_FLUID && i > 0 && i < nx - 1 && urow > 0 && urow < ny - 1) {
-                const float *T0 = Tq + (size_t)((urow % TR + TR) % TR) * 5 * NT;
-                const float *TN = Tq + (size_t)(((urow + 1) % TR + TR) % TR) * 5 * NT;
-                const float *TS = Tq + (size_t)(((urow - 1) % TR + TR) % TR) * 5 * NT;
+            const float4 pc = P[p2 * NT + c];
+            if (ctype == CT_FLUID && interior_x && urow > 0 && urow < ny - 1) {
+                const float *T0 = Tq + s2 * 5 * NT + tc;
+                const float *TN = Tq + s1 * 5 * NT + tc;
+                const float *TS = Tq + s3 * 5 * NT + tc;
                 float tC[5], tE[5], tW[5], tNn[5], tSs[5];
 #pragma unroll
                 for (int k = 0; k < 5; k++) {
-                    tC[k] = T0[k * NT + tc];
-                    tE[k] = T0[k * NT + tc + 1];
-                    tW[k] = T0[k * NT + tc - 1];
-                    tNn[k] = TN[k * NT + tc];
-                    tSs[k] = TS[k * NT + tc];
+                    tC[k] = T0[k * NT];
+                    tE[k] = T0[k * NT + 1];
+                    tW[k] = T0[k * NT - 1];
+                    tNn[k] = TN[k * NT];
+                    tSs[k] = TS[k * NT];
                 }
-                const float4 E = P[su * NT + c + 1], Wc = P[su * NT + c - 1];
-                const float4 N = P[((urow + 1) % PR + PR) % PR * NT + c];
-                const float4 S = P[((urow - 1) % PR + PR) % PR * NT + c];
+                const float4 E = P[p2 * NT + c + 1], Wc = P[p2 * NT + c - 1];
+                const float4 N = P[p1 * NT + c];
+                const float4 S = P[p3 * NT + c];
                 float rhs[4];
                 viscous_rhs(tC, tE, tW, tNn, tSs, E.x, Wc.x, N.x, S.x, E.y, Wc.y, N.y, S.y, va, rhs);
                 U[1] += dt * rhs[0];
@@ -451,7 +480,7 @@ __global__ void __launch_bounds__(NT) k_viscous(const __grid_constant__ CUtensor
                 U[3] += dt * rhs[2];
                 U[4] += dt * rhs[3];
             }
-            if (a.apply_bc) bc_pointwise(U, ctype, i, urow, nx, ny, a.fs);
+            if (a.apply_bc) bc_pointwise(U, ctype, iu, urow, nx, ny, a.fs);
             if (a.cfl && ctype != CT_GHOST) {
                 float uu, vv, pp, TT;
                 prim_from_cons(U[0], U[1], U[2], U[3], U[4], uu, vv, pp, TT);
@@ -461,10 +490,20 @@ __global__ void __launch_bounds__(NT) k_viscous(const __grid_constant__ CUtensor
                     lmax_nu = fmaxf(lmax_nu, mu / (U[0] + 1e-10f));
                 }
             }
-            float *dst = a.out + (size_t)urow * g.pitch + i;
+            float *dst = outp + (size_t)urow * g.pitch;
 #pragma unroll
             for (int k = 0; k < 5; k++) dst[k * g.plane] = U[k];
         }
+        kr = ring_next<K>(kr);
+        par ^= (kr == 0) ? 1 : 0;
+        ku = ring_next<K>(ku);
+        p3 = p2;
+        p2 = p1;
+        p1 = p0;
+        p0 = ring_next<PR>(p0);
+        s3 = s2;
+        s2 = s1;
+        s1 = ring_next<TR>(s1);
     }
     if (aborted) {
         if (t == 0) {

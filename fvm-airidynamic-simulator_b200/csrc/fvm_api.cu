@@ -179,9 +179,11 @@ struct fvm_handle {
     StageTune tune{128, 6, 32};
     bool dt_ready = false;       // recompute policy: sc->dt holds the next dt
     bool cfl_valid = false;      // sc->cfl holds the maxima of the current state
-    // graph replay of two steps
-    cudaGraphExec_t graph = nullptr;
-    unsigned long long graph_key = 0;
+    // graph replay of two steps, one per buffer parity (which of the two
+    // ping-pong buffers currently holds U^n)
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    unsigned long long graph_key[2] = {0, 0};
+    float *parity_base = nullptr;  // buffer holding U^n at parity 0
     // measurement
     bool timing = false;
     std::vector<TimedLaunch> pending;
@@ -237,11 +239,16 @@ static cudaError_t timed(fvm_handle *h, int kernel, F fn) {
     return e;
 }
 
-static void free_buffers(fvm_handle *h) {
-    if (h->graph) {
-        cudaGraphExecDestroy(h->graph);
-        h->graph = nullptr;
+static void drop_graphs(fvm_handle *h) {
+    for (int k = 0; k < 2; k++) {
+        if (h->graph[k]) cudaGraphExecDestroy(h->graph[k]);
+        h->graph[k] = nullptr;
+        h->graph_key[k] = 0;
     }
+}
+
+static void free_buffers(fvm_handle *h) {
+    drop_graphs(h);
     for (int k = 0; k < NBUF; k++) {
         if (h->buf[k]) cudaFree(h->buf[k]);
         h->buf[k] = nullptr;
@@ -258,6 +265,7 @@ static void free_buffers(fvm_handle *h) {
     h->d_diag = nullptr;
     h->n_ghost = h->ghost_cap = 0;
     h->bytes = 0;
+    h->parity_base = nullptr;
 }
 
 // Tuning per grid class: rows per CTA so that the launch covers ~6 CTAs per
@@ -364,10 +372,7 @@ static int build_geometry(fvm_handle *h, bool fixup) {
     if (n > 0) launch_ghost_table(h->g, h->sdf, h->ct, h->ghosts, h->ghost_cap, h->d_count, h->stream);
     CK(cudaGetLastError());
     h->n_ghost = n;
-    if (h->graph) {
-        cudaGraphExecDestroy(h->graph);
-        h->graph = nullptr;
-    }
+    drop_graphs(h);
     return FVM_OK;
 }
 
@@ -447,10 +452,7 @@ extern "C" int fvm_set_stream(fvm_handle *h, void *stream) {
     CHECK_HANDLE(h);
     cudaStreamSynchronize(h->stream);
     h->stream = stream ? reinterpret_cast<cudaStream_t>(stream) : h->own;
-    if (h->graph) {
-        cudaGraphExecDestroy(h->graph);
-        h->graph = nullptr;
-    }
+    drop_graphs(h);
     return FVM_OK;
 }
 
@@ -515,10 +517,7 @@ extern "C" int fvm_set_ext(fvm_handle *h, const fvm_ext *ext) {
     if (int r = validate(&h->prm, ext)) return r;
     if (!ext) return set_err(FVM_ERR_INVALID, "null ext");
     h->ext = *ext;
-    if (h->graph) {
-        cudaGraphExecDestroy(h->graph);
-        h->graph = nullptr;
-    }
+    drop_graphs(h);
     h->dt_ready = false;
     return FVM_OK;
 }
@@ -643,6 +642,11 @@ static unsigned long long graph_key(fvm_handle *h) {
     k = k * 1000003ULL + (unsigned long long)h->n_ghost;
     k = k * 7 + h->ext.dt_policy;
     k = k * 1000003ULL + (unsigned long long)(uintptr_t)h->stream;
+    uint32_t c1, c2;
+    memcpy(&c1, &h->prm.cfl, 4);
+    memcpy(&c2, &h->prm.cfl_visc, 4);
+    k = k * 1000003ULL + c1;
+    k = k * 1000003ULL + c2;
     return k;
 }
 
@@ -684,22 +688,22 @@ extern "C" int fvm_steps(fvm_handle *h, fvm_sim_params *p, int n) {
         h->prm.enable_viscosity = p->enable_viscosity;
         h->prm.adiabatic_wall = p->adiabatic_wall;
         h->prm.T_wall = p->T_wall;
-        if (h->graph) {
-            cudaGraphExecDestroy(h->graph);
-            h->graph = nullptr;
-        }
+        drop_graphs(h);
     }
     if (int r = prepare_dt(h, p)) return r;
     const bool use_graph = !h->timing && n >= 2 && h->stream != nullptr && h->stream != cudaStreamLegacy &&
                            h->stream != cudaStreamPerThread && getenv("FVM_NO_GRAPH") == nullptr;
     int done = 0;
-    if (use_graph) {
+    if (use_graph && n >= 2) {
+        // the captured pointers depend on which ping-pong buffer holds U^n
+        if (!h->parity_base) h->parity_base = h->buf[BUF_N];
+        const int par = (h->buf[BUF_N] == h->parity_base) ? 0 : 1;
         unsigned long long key = graph_key(h);
-        if (h->graph && h->graph_key != key) {
-            cudaGraphExecDestroy(h->graph);
-            h->graph = nullptr;
+        if (h->graph[par] && h->graph_key[par] != key) {
+            cudaGraphExecDestroy(h->graph[par]);
+            h->graph[par] = nullptr;
         }
-        if (!h->graph) {
+        if (!h->graph[par]) {
             cudaGraph_t gr;
             CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
             long long before = h->launches;
@@ -711,14 +715,14 @@ extern "C" int fvm_steps(fvm_handle *h, fvm_sim_params *p, int n) {
             h->launches = before;
             if (r1 || r2) return r1 ? r1 : r2;
             CK(ec);
-            cudaError_t ei = cudaGraphInstantiate(&h->graph, gr, 0);
+            cudaError_t ei = cudaGraphInstantiate(&h->graph[par], gr, 0);
             cudaGraphDestroy(gr);
             CK(ei);
-            h->graph_key = key;
+            h->graph_key[par] = key;
         }
         const int per_step = h->prm.enable_viscosity ? 6 : 4;
         for (; done + 2 <= n; done += 2) {
-            CK(cudaGraphLaunch(h->graph, h->stream));
+            CK(cudaGraphLaunch(h->graph[par], h->stream));
             h->launches += 2 * per_step;
         }
     }

@@ -1,0 +1,248 @@
+"""The reference-facing surface of the library on a GPU (through the C ABI):
+readback/writeback, derived fields, statistics, arrows, obstacle updates,
+checkpoint/restore, determinism, graph replay, errors, diagnostics, the
+CFDSolver shim benchmark."""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from helpers import REPO, small, rel_l1, rel_linf, FIELDS
+
+pytestmark = pytest.mark.gpu
+
+import fvm_b200  # noqa: E402
+from fvm_b200 import Solver, FvmError, abi  # noqa: E402
+from oracle.oracle import Oracle  # noqa: E402
+
+
+def _solver(name="euler_m3_circle", nx=160, ny=80, **kw):
+    p, e = small(name, nx, ny, **kw)
+    return Solver(p, e), p, e
+
+
+def test_fields_roundtrip_bitwise():
+    s, p, _ = _solver()
+    rng = np.random.default_rng(7)
+    U = s.fields()
+    U = (U * (1.0 + 0.01 * rng.standard_normal(U.shape))).astype(np.float32)
+    s.write_fields(U)
+    assert np.array_equal(s.fields().view(np.uint32), U.view(np.uint32))
+
+
+def test_primitives_match_oracle_formula():
+    s, p, e = _solver()
+    s.step(5)
+    o = Oracle(p, e, bits=32)
+    o.set_fields(s.fields())
+    prim = s.primitives()
+    ref = o.primitives()
+    for k in range(4):
+        assert np.allclose(prim[k], ref[k], rtol=2e-6, atol=1e-6 * np.abs(ref[k]).max())
+
+
+def test_derived_fields_to_device():
+    torch = pytest.importorskip("torch")
+    s, p, _ = _solver()
+    s.step(3)
+    U = s.fields().astype(np.float64)
+    rho, ru, rv, rE = U[0], U[1], U[2], U[4]
+    rv_ = rho + 1e-10
+    u, v = ru / rv_, rv / rv_
+    T = 0.4 * (rE / rv_) / 287.05
+    expect = {
+        abi.FIELD_TEMPERATURE: T, abi.FIELD_PRESSURE: 0.4 * rE, abi.FIELD_DENSITY: rho,
+        abi.FIELD_VELOCITY_MAG: np.hypot(u, v), abi.FIELD_MACH: np.hypot(u, v) / (np.sqrt(1.4 * 287.05 * T) + 1e-10),
+    }
+    buf = torch.empty(p.nx * p.ny, dtype=torch.float32, device="cuda")
+    for kind, ref in expect.items():
+        s.field_to_device(kind, buf.data_ptr())
+        torch.cuda.synchronize()
+        got = buf.cpu().numpy().reshape(p.ny, p.nx)
+        assert np.allclose(got, ref, rtol=1e-5), kind
+    s.cell_types_to_device(buf.data_ptr())
+    torch.cuda.synchronize()
+    assert np.array_equal(buf.cpu().numpy().reshape(p.ny, p.nx), s.cell_types().astype(np.float32))
+
+
+def test_max_temperature_and_mach():
+    s, p, _ = _solver()
+    s.step(10)
+    u, v, pr, T = s.primitives().astype(np.float64)
+    rho = s.fields()[0].astype(np.float64)
+    assert s.max_temperature() == pytest.approx(T.max(), rel=1e-6)
+    mach = np.hypot(u, v) / (np.sqrt(1.4 * pr / (rho + 1e-10)) + 1e-10)
+    assert s.max_mach() == pytest.approx(mach.max(), rel=1e-5)
+
+
+def test_vector_arrows_count_and_geometry():
+    torch = pytest.importorskip("torch")
+    s, p, _ = _solver()
+    s.step(5)
+    step = 8
+    cap = 100000
+    vb = torch.zeros(cap * 5, dtype=torch.float32, device="cuda")
+    n = s.vector_arrows(vb.data_ptr(), cap, step, p.u_inf, 0.05, 0.5, 0.3)
+    u, v, _, _ = s.primitives()
+    js = np.arange(step // 2, p.ny, step)
+    is_ = np.arange(step // 2, p.nx, step)
+    sp = np.hypot(u[np.ix_(js, is_)], v[np.ix_(js, is_)])
+    assert n == 8 * int((sp >= 1e-6 * p.u_inf).sum())
+    verts = vb.cpu().numpy()[: (n // 8) * 40].reshape(-1, 8, 5)
+    assert np.all(np.abs(verts[:, :6, :2]) <= 1.2)
+    # tail at the sample point, head length <= max length
+    length = np.hypot(verts[:, 1, 0] - verts[:, 0, 0], verts[:, 1, 1] - verts[:, 0, 1])
+    assert np.all(length <= 0.05 + 1e-6)
+    # a capacity smaller than the arrow count writes nothing past it
+    vb2 = torch.full((40 * 5,), -7.0, dtype=torch.float32, device="cuda")
+    n2 = s.vector_arrows(vb2.data_ptr(), 16, step, p.u_inf, 0.05, 0.5, 0.3)
+    assert n2 == n
+
+
+def test_update_obstacle_matches_oracle():
+    s, p, e = _solver(nx=192, ny=96)
+    o = Oracle(p, e, bits=32)
+    o.set_geometry(s.sdf(), s.cell_types())
+    o.set_fields(s.fields())
+    dt = o.compute_dt()
+    p.dt = dt
+    s.step(10)
+    for _ in range(10):
+        o.step(dt)
+    q = abi.SimParams.from_buffer_copy(p)
+    q.obstacle_x = p.obstacle_x + 3.5 * p.dx
+    q.obstacle_r = p.obstacle_r * 0.8
+    s.update_obstacle(q)
+    o.update_obstacle(q)
+    _, oct_ = o.geometry()
+    assert (s.cell_types() != oct_).sum() <= 2
+    o.set_geometry(s.sdf(), s.cell_types())
+    assert rel_l1(s.fields(), o.fields()).max() < 1e-4
+
+
+def test_checkpoint_restore_is_bitwise():
+    s, p, e = _solver()
+    p.dt = s.compute_dt()
+    s.step(7)
+    ckpt = s.fields()
+    s.step(9)
+    a = s.fields()
+    s2 = Solver(abi.SimParams.from_buffer_copy(p), e)
+    s2.params.dt = p.dt
+    s2.write_fields(ckpt)
+    s2.step(9)
+    assert np.array_equal(a.view(np.uint32), s2.fields().view(np.uint32))
+
+
+def test_runs_are_deterministic_and_graph_replay_matches_single_steps():
+    outs = []
+    for mode in ("graph", "graph", "single"):
+        s, p, e = _solver("ns_karman_re200", 160, 80)
+        p.dt = s.compute_dt()
+        if mode == "graph":
+            s.step(12)
+        else:
+            for _ in range(12):
+                s.step(1)
+        outs.append(s.fields())
+    assert np.array_equal(outs[0].view(np.uint32), outs[1].view(np.uint32))
+    assert np.array_equal(outs[0].view(np.uint32), outs[2].view(np.uint32))
+
+
+def test_compute_dt_matches_oracle():
+    for name in ("euler_m3_circle", "ns_karman_re200"):
+        s, p, e = _solver(name)
+        o = Oracle(p, e, bits=64)
+        o.set_geometry(s.sdf(), s.cell_types())
+        o.set_fields(s.fields())
+        assert s.compute_dt() == pytest.approx(o.compute_dt(), rel=2e-6)
+
+
+def test_errors_are_status_codes():
+    p, e = small("euler_m3_circle", 64, 32)
+    s = Solver()
+    with pytest.raises(FvmError) as ei:
+        s.params = p
+        s.step(1)
+    assert ei.value.code == 4
+    bad = abi.SimParams.from_buffer_copy(p)
+    bad.nx = 0
+    with pytest.raises(FvmError) as ei:
+        s.initialize(bad, e)
+    assert ei.value.code == 1
+    e2 = abi.Ext.from_buffer_copy(e)
+    e2.flux_scheme = 9
+    with pytest.raises(FvmError) as ei:
+        s.initialize(p, e2)
+    assert ei.value.code == 1
+    s.initialize(p, e)
+    assert s.memory_usage() > p.nx * p.ny * 60
+    free, total = fvm_b200.gpu_mem_info()
+    assert 0 < free <= total
+
+
+def test_kernel_timing_and_launch_counts():
+    s, p, e = _solver()
+    p.dt = s.compute_dt()
+    n0 = s.launch_count()
+    s.set_kernel_timing(True)
+    s.step(4)
+    s.synchronize()
+    kt = s.kernel_times()
+    assert set(kt) >= {"stage1", "stage2", "ghost1", "ghost2"}
+    assert all(v[0] == 4 for k, v in kt.items() if k.startswith("stage"))
+    assert s.launch_count() - n0 >= 16
+
+
+def test_external_stream():
+    torch = pytest.importorskip("torch")
+    s, p, e = _solver()
+    p.dt = s.compute_dt()
+    st = torch.cuda.Stream()
+    s.set_stream(st.cuda_stream)
+    s.step(6)
+    a = s.fields()
+    s2, p2, _ = _solver()
+    p2.dt = p.dt
+    s2.step(6)
+    assert np.array_equal(a.view(np.uint32), s2.fields().view(np.uint32))
+
+
+@pytest.mark.parametrize("name", ["euler_m3_circle", "ns_karman_re200"])
+def test_diagnostics_match_oracle(name):
+    s, p, e = _solver(name, 192, 96)
+    o = Oracle(p, e, bits=64)
+    o.set_geometry(s.sdf(), s.cell_types())
+    o.set_fields(s.fields())
+    dt = o.compute_dt()
+    p.dt = dt
+    s.step(20)
+    for _ in range(20):
+        o.step(dt)
+    o.set_fields(s.fields())  # same state: compare the reductions themselves
+    d, r = s.diagnostics(), o.diagnostics()
+    for f in ("force_x", "force_y", "mass", "mom_x", "energy", "wall_heat"):
+        a, b = getattr(d, f), getattr(r, f)
+        assert a == pytest.approx(b, rel=1e-4, abs=1e-9 * max(1.0, abs(b))), f
+    assert d.cd == pytest.approx(r.cd, rel=1e-4, abs=1e-9)
+
+
+def test_shock_standoff_matches_oracle():
+    s, p, e = _solver("euler_m3_circle", 256, 128)
+    p.dt = s.compute_dt()
+    s.step(300)
+    o = Oracle(p, e, bits=64)
+    o.set_geometry(s.sdf(), s.cell_types())
+    o.set_fields(s.fields())
+    a, b = s.shock_standoff(), o.shock_standoff()
+    assert np.isfinite(a) and a > 0
+    assert a == pytest.approx(b, rel=1e-5)
+
+
+def test_shim_kernel_benchmark_runs():
+    exe = os.path.join(REPO, "fvm-airidynamic-simulator_b200", "fvm_b200", "lib", "kernel_benchmark")
+    out = subprocess.run([exe, "256", "128", "5"], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stderr
+    assert "Avg per step" in out.stdout

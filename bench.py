@@ -201,6 +201,7 @@ def main():
     ap.add_argument("--nx", type=int, default=0)
     ap.add_argument("--ny", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="skip the launch-shape autotuner")
     args = ap.parse_args()
     assert args.warmup >= 3, "at least 3 warm-up steps"
 
@@ -225,6 +226,8 @@ def main():
         # settle into a non-uniform flow, fixed dt from the start state
         params.dt = s.compute_dt()
         s.step(args.settle)
+        if not args.no_autotune:
+            s.autotune(steps=4)  # launch shape for this grid class (untimed)
         s.step(args.warmup)
         torch.cuda.synchronize()
 
@@ -301,7 +304,8 @@ def main():
             "config": {"workload": args.workload, "nx": nx, "ny": ny,
                        "viscous": bool(params.enable_viscosity),
                        "flux": ["hllc", "ausm+"][ext.flux_scheme], "limiter": ["minmod", "van_leer"][ext.limiter],
-                       "parallelism": f"replicas x{ws}", "l2": "inputs > L2 (670 MB per state), no flush"},
+                       "parallelism": f"replicas x{ws}", "l2": "inputs > L2 (670 MB per state), no flush",
+                       "tune": dict(zip(("threads", "ring", "rows_per_cta"), s.tune()))},
             "hbm_gbs_per_gpu_at_102B": step_gbs,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": traffic, "kernel": dom_name,

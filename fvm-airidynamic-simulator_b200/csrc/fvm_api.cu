@@ -13,6 +13,7 @@
 #include <cstring>
 #include <map>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/fvm_b200.h"
@@ -268,27 +269,43 @@ static void free_buffers(fvm_handle *h) {
     h->parity_base = nullptr;
 }
 
-// Tuning per grid class: rows per CTA so that the launch covers ~6 CTAs per
-// SM; FVM_TUNE="nt,ring,rows" overrides (used by the autotuner sweep).
-static StageTune pick_tune(int nx, int ny) {
-    StageTune t{128, 6, 32};
+// Launch tuning of the marching kernels per grid class.  Default: 128
+// threads, 6-slot ring, rows per CTA chosen so a launch spans ~6 waves of
+// the 148 SMs x ~5 resident CTAs (short enough rows to balance the last
+// wave, long enough to amortise the 4-row halo).  FVM_TUNE="nt,ring,rows"
+// overrides; fvm_autotune measures the candidates and caches the winner per
+// grid class for the process.
+struct TuneKey {
+    int nx, ny, viscous, scheme, limiter;
+    bool operator<(const TuneKey &o) const {
+        return std::tie(nx, ny, viscous, scheme, limiter) < std::tie(o.nx, o.ny, o.viscous, o.scheme, o.limiter);
+    }
+};
+static std::map<TuneKey, StageTune> g_tune_cache;
+
+static StageTune heuristic_tune(int nx, int ny) {
+    StageTune t{128, 6, 64};
+    int strips = (nx + t.nt - 5) / (t.nt - 4);
+    long long target = 148LL * 5 * 6;
+    int rows = (int)((long long)ny * strips / target);
+    rows = std::max(16, std::min(128, rows));
+    t.rows = (rows + 7) / 8 * 8;
+    return t;
+}
+
+static StageTune pick_tune(const fvm_handle *h, int nx, int ny);
+
+static StageTune pick_tune(const fvm_handle *h, int nx, int ny) {
     const char *env = getenv("FVM_TUNE");
     if (env) {
-        int a = 0, b = 0, c = 0;
-        if (sscanf(env, "%d,%d,%d", &a, &b, &c) == 3 && (a == 128 || a == 256) && (b == 6 || b == 8) && c >= 4) {
-            t.nt = a;
-            t.ring = b;
-            t.rows = c;
-            return t;
-        }
+        int x = 0, y = 0, z = 0;
+        if (sscanf(env, "%d,%d,%d", &x, &y, &z) == 3 && (x == 128 || x == 256) && (y == 6 || y == 8) && z >= 4)
+            return StageTune{x, y, z};
     }
-    int strips = (nx + t.nt - 5) / (t.nt - 4);
-    long long target = 148LL * 6;
-    int rows = (int)((long long)ny * strips / target);
-    rows = std::max(8, std::min(256, rows));
-    rows = (rows + 7) / 8 * 8;
-    t.rows = rows;
-    return t;
+    TuneKey k{nx, ny, h->prm.enable_viscosity ? 1 : 0, h->ext.flux_scheme, h->ext.limiter};
+    auto it = g_tune_cache.find(k);
+    if (it != g_tune_cache.end()) return it->second;
+    return heuristic_tune(nx, ny);
 }
 
 static int alloc_buffers(fvm_handle *h, int nx, int ny) {
@@ -313,7 +330,7 @@ static int alloc_buffers(fvm_handle *h, int nx, int ny) {
     h->diag_parts = diagnostics_parts(g);
     CKA(cudaMalloc(&h->d_diag, (size_t)(h->diag_parts * 8 + 16) * sizeof(double)));
     h->bytes = state_bytes * NBUF + (size_t)g.plane * 5 + (size_t)nx * ny + (size_t)(h->diag_parts * 8 + 16) * 8;
-    h->tune = pick_tune(nx, ny);
+    h->tune = pick_tune(h, nx, ny);
     return FVM_OK;
 }
 
@@ -991,6 +1008,77 @@ extern "C" int fvm_launch_count(fvm_handle *h, long long *count_out) {
     CHECK_HANDLE(h);
     if (!count_out) return set_err(FVM_ERR_INVALID, "null output");
     *count_out = h->launches;
+    return FVM_OK;
+}
+
+// Time each candidate tuning over `steps` steps from a snapshot of the
+// current state (restored after every candidate) and keep the fastest.
+extern "C" int fvm_autotune(fvm_handle *h, const fvm_sim_params *p, int steps, float *best_ms_out) {
+    CHECK_INIT(h);
+    if (!p || steps < 2) return set_err(FVM_ERR_INVALID, "fvm_autotune: need params and steps >= 2");
+    const size_t bytes = (size_t)h->g.plane * 5 * sizeof(float);
+    float *snap = nullptr;
+    CKA(cudaMalloc(&snap, bytes));
+    CK(cudaMemcpyAsync(snap, h->buf[BUF_N], bytes, cudaMemcpyDeviceToDevice, h->stream));
+    const StageTune before = h->tune;
+    const bool timing = h->timing;
+    h->timing = false;
+    fvm_sim_params q = *p;
+    StageTune best = before;
+    float best_ms = 1e30f;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int rc = FVM_OK;
+    const int nts[2] = {128, 256}, rings[2] = {6, 8}, rows[5] = {16, 32, 64, 128, 256};
+    for (int a1 = 0; a1 < 2 && rc == FVM_OK; a1++)
+        for (int a2 = 0; a2 < 2 && rc == FVM_OK; a2++)
+            for (int a3 = 0; a3 < 5 && rc == FVM_OK; a3++) {
+                StageTune cand{nts[a1], rings[a2], rows[a3]};
+                if (rows[a3] > std::max(16, h->g.ny)) continue;
+                h->tune = cand;
+                drop_graphs(h);
+                if ((rc = build_maps(h)) != FVM_OK) break;
+                fvm_sim_params w = q;
+                if ((rc = fvm_steps(h, &w, 2)) != FVM_OK) break;  // warm (graph capture)
+                cudaEventRecord(e0, h->stream);
+                if ((rc = fvm_steps(h, &w, steps)) != FVM_OK) break;
+                cudaEventRecord(e1, h->stream);
+                cudaEventSynchronize(e1);
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                ms /= steps;
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best = cand;
+                }
+                // restore the state for the next candidate (buffer roles may have swapped)
+                cudaMemcpyAsync(h->buf[BUF_N], snap, bytes, cudaMemcpyDeviceToDevice, h->stream);
+            }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    h->tune = (rc == FVM_OK) ? best : before;
+    drop_graphs(h);
+    int r2 = build_maps(h);
+    cudaMemcpyAsync(h->buf[BUF_N], snap, bytes, cudaMemcpyDeviceToDevice, h->stream);
+    cudaStreamSynchronize(h->stream);
+    cudaFree(snap);
+    h->timing = timing;
+    h->cfl_valid = false;
+    h->dt_ready = false;
+    if (rc != FVM_OK) return rc;
+    if (r2 != FVM_OK) return r2;
+    g_tune_cache[TuneKey{h->g.nx, h->g.ny, h->prm.enable_viscosity ? 1 : 0, h->ext.flux_scheme, h->ext.limiter}] =
+        best;
+    if (best_ms_out) *best_ms_out = best_ms;
+    return FVM_OK;
+}
+
+extern "C" int fvm_get_tune(fvm_handle *h, int *nt, int *ring, int *rows) {
+    CHECK_INIT(h);
+    if (nt) *nt = h->tune.nt;
+    if (ring) *ring = h->tune.ring;
+    if (rows) *rows = h->tune.rows;
     return FVM_OK;
 }
 

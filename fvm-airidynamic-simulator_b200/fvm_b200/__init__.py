@@ -28,7 +28,7 @@ EXPORTS = [
     "fvm_write_fields", "fvm_read_primitives", "fvm_field_to_device", "fvm_cell_types_to_device",
     "fvm_vector_arrows", "fvm_max_temperature", "fvm_max_mach", "fvm_memory_usage", "fvm_gpu_mem_info",
     "fvm_diagnostics", "fvm_shock_standoff", "fvm_set_kernel_timing", "fvm_kernel_times",
-    "fvm_launch_count", "fvm_debug_stage1", "fvm_debug_ghost_table", "fvm_build_info",
+    "fvm_launch_count", "fvm_autotune", "fvm_get_tune", "fvm_debug_stage1", "fvm_debug_ghost_table", "fvm_build_info",
 ]
 
 
@@ -93,6 +93,8 @@ def load_library(path=None):
     lib.fvm_kernel_times.argtypes = [vp, C.POINTER(KernelTime), i, C.POINTER(i)]
     lib.fvm_launch_count.argtypes = [vp, C.POINTER(C.c_longlong)]
     lib.fvm_debug_stage1.argtypes = [vp, f, i] + [vp] * 5
+    lib.fvm_autotune.argtypes = [vp, Pp, i, fp]
+    lib.fvm_get_tune.argtypes = [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i)]
     lib.fvm_debug_ghost_table.argtypes = [vp, vp, i, C.POINTER(i)]
     _lib = lib
     return lib
@@ -266,6 +268,17 @@ class Solver:
         out = np.zeros((max(n.value, 1), 7), np.int32)
         _check(self.lib.fvm_debug_ghost_table(self.h, _p(out), n.value, C.byref(n)))
         return out[:n.value]
+
+    def autotune(self, steps=6):
+        """Pick the fastest launch tuning for this grid class (see fvm_autotune)."""
+        ms = C.c_float()
+        _check(self.lib.fvm_autotune(self.h, C.byref(self.params), int(steps), C.byref(ms)))
+        return ms.value
+
+    def tune(self):
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        _check(self.lib.fvm_get_tune(self.h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
 
     def launch_count(self):
         v = C.c_longlong()

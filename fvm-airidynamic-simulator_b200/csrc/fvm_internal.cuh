@@ -46,6 +46,8 @@ struct DevScalars {
     unsigned err;     // error word (kErrTimeout, kErrNonFinite)
     unsigned nonfinite;
     float dt_last;    // dt of the last completed step (recompute policy)
+    unsigned parity;  // batched solves: which ping-pong buffer holds U^n
+    unsigned pad;
     double diag[16];  // FP64 diagnostic accumulators
 };
 
@@ -80,6 +82,42 @@ struct GhostArgs {
     int recompute_dt;
     float cfl_num, cfl_visc, min_dx;
     int viscous;
+    int flip_parity;       // batched solves: toggle sc->parity in the finalize
+};
+
+// ---------------------------------------------------------- batched solves
+// Buffer roles of a solve's state buffers.  Physical buffers 0 and 2 hold
+// U^n / U^{n+1} alternately (DevScalars::parity), 1 holds U*, 3 holds
+// U_d / U_b of the viscous path.
+enum { ROLE_N = 0, ROLE_S = 1, ROLE_X = 2, ROLE_D = 3 };
+
+// Per-instance descriptor of a batch (device memory; TMA maps must be 64-byte
+// aligned).
+struct alignas(64) BatchInst {
+    CUtensorMap tm_in[4];   // halo'd row boxes, per physical buffer
+    CUtensorMap tm_ctr[4];  // blend-partner boxes, per physical buffer
+    float *buf[4];
+    GridDesc g;
+    const uint8_t *mask;
+    DevScalars *sc;
+    Freestream fs;
+    WallParams wall;
+    float prandtl;
+    int ref_prandtl;
+    int viscous;
+    const GhostInfo *ghosts;
+    int n_ghost;
+    int n_gchunks;
+    int recompute_dt;
+    float cfl_num, cfl_visc, min_dx;
+};
+
+struct TileDesc {
+    int inst, i0, j0, pad;
+};
+
+struct GhostChunk {
+    int inst, first, count, pad;
 };
 
 }  // namespace fvm

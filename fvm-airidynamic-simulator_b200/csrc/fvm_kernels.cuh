@@ -34,6 +34,13 @@ cudaError_t launch_stage(int stage, int scheme, int limiter, const StageTune &tn
 // Viscous half step out of place: out = U + dt*D(prims(U)) on interior fluid
 // cells, copy elsewhere; optional phase-1 BC and CFL reduction.
 cudaError_t launch_viscous(const StageTune &tn, const CUtensorMap &tm_in, const StepArgs &a, cudaStream_t st);
+// Batched launches over a multi-instance tile list (persistent grids).
+cudaError_t launch_stage_batch(int stage, int scheme, int limiter, const StageTune &tn, const BatchInst *insts,
+                               const TileDesc *tiles, int ntiles, cudaStream_t st);
+cudaError_t launch_viscous_batch(const StageTune &tn, const BatchInst *insts, const TileDesc *tiles, int ntiles,
+                                 int post, cudaStream_t st);
+cudaError_t launch_ghost_batch(const BatchInst *insts, const GhostChunk *chunks, int nchunks, int mode,
+                               cudaStream_t st);
 // Ghost-cell pass over the ghost table.
 cudaError_t launch_ghost(const GhostArgs &a, cudaStream_t st);
 // Phase-1 boundary conditions in place on a whole state (set-up path).

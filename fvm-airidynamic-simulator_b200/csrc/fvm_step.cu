@@ -15,6 +15,7 @@
 // crosses HBM once (halo re-reads hit L2).  Domain-edge halos use the
 // reference's clamp-to-edge semantics (src/solver.cu:1484-1488): rows by
 // clamping the TMA row coordinate, columns by clamping the shared-memory column.
+#include <algorithm>
 #include <cstdio>
 
 #include "fvm_kernels.cuh"
@@ -107,18 +108,24 @@ __device__ __forceinline__ int ring_next(int s) {
     return (s + 1 == N) ? 0 : s + 1;
 }
 
-// Inviscid SSP-RK2 stage (computeFluxesKernel + updateKernel + [blend] +
-// phase-1 BC, src/solver.cu:1450-1876, :949-967, :1891-2042).
+// TMA ring position carried across the tiles a CTA processes: `base` counts
+// rows staged so far; slot = base % K and the mbarrier phase parity is
+// (base / K) & 1 for the row staged at `base`.
+struct RingPos {
+    int base;
+};
+
+// Inviscid SSP-RK2 stage on one tile (strip [i0, i0+W) x rows [j0, j1))
+// (computeFluxesKernel + updateKernel + [blend] + phase-1 BC,
+// src/solver.cu:1450-1876, :949-967, :1891-2042).  Returns false when a
+// bounded wait expired (error recorded; caller must stop).
 template <int NT, int K, int STAGE, int SCHEME, int LIM>
-__global__ void __launch_bounds__(NT) k_stage(const __grid_constant__ CUtensorMap tm_in,
-                                              const __grid_constant__ CUtensorMap tm_blend, const StepArgs a) {
+__device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUtensorMap *tm_blend, const StepArgs &a,
+                                           int i0, int j0, unsigned char *smem, RingPos &rp, float &lmax_speed) {
     using L = StageLayout<NT, K, STAGE>;
     constexpr int W = L::W, PR = L::PR, XR = L::XR;
-    static_assert(L::total <= 227 * 1024, "shared memory");
     static_assert(PR == 5 && XR == 3, "ring sizes");
     constexpr int AHEAD = K - 3;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    unsigned char *smem = aligned_smem(smem_raw);
     float *raw = reinterpret_cast<float *>(smem + L::raw_off);
     float *bl = reinterpret_cast<float *>(smem + L::bl_off);
     float4 *P = reinterpret_cast<float4 *>(smem + L::p_off);
@@ -130,56 +137,47 @@ __global__ void __launch_bounds__(NT) k_stage(const __grid_constant__ CUtensorMa
     const GridDesc g = a.g;
     const int nx = g.nx, ny = g.ny;
     const int t = threadIdx.x;
-    const int i0 = blockIdx.x * W;
-    const int j0 = blockIdx.y * a.rows_per_cta;
     const int j1 = min(j0 + a.rows_per_cta, ny);
     const int rs = j0 - 2;
     const int nrows = (j1 + 1) - rs + 1;  // incoming rows rs .. j1+1
-
     const float dt = a.sc->dt * a.dt_scale;
     const UpdateArgs ua{dt, 1.0f / g.dx, 1.0f / g.dy};
 
-    if (t == 0) {
-        prefetch_tensormap(&tm_in);
-        if (STAGE == 2) prefetch_tensormap(&tm_blend);
-        for (int k = 0; k < K; k++) mbar_init(&bars[k], 1);
-        fence_barrier_init();
-    }
+    // slots of the previous tile are free once every thread is past its last read
+    fence_proxy_async_smem();
     __syncthreads();
+    const int base = rp.base;
+    int islot = base % K;
     auto issue = [&](int q) {
-        const int slot = q % K;
         const int row = clampi(rs + q, 0, ny - 1);
-        mbar_arrive_expect_tx(&bars[slot], L::tx_bytes);
+        mbar_arrive_expect_tx(&bars[islot], L::tx_bytes);
 #pragma unroll
         for (int b = 0; b < L::NB; b++)
-            tma_load_3d(raw + (size_t)slot * L::SLOT + b * kBoxStride, &tm_in, &bars[slot], i0 - 4 + b * kBox, row, 0);
-        if (STAGE == 2) tma_load_3d(bl + (size_t)slot * L::BSLOT, &tm_blend, &bars[slot], i0, row, 0);
+            tma_load_3d(raw + (size_t)islot * L::SLOT + b * kBoxStride, tm_in, &bars[islot], i0 - 4 + b * kBox, row,
+                        0);
+        if (STAGE == 2) tma_load_3d(bl + (size_t)islot * L::BSLOT, tm_blend, &bars[islot], i0, row, 0);
+        islot = ring_next<K>(islot);
     };
-    if (t == 0)
-        for (int q = 0; q < min(AHEAD, nrows); q++) issue(q);
-
-    float lmax_speed = 0.0f;
     int issued = min(AHEAD, nrows);
-    bool aborted = false;
-    // mask bytes of this thread's column, prefetched two rows ahead
+    if (t == 0)
+        for (int q = 0; q < issued; q++) issue(q);
+
     const int ic_t = clampi(i0 - 2 + t, 0, nx - 1);
     const int rc_t = ic_t - i0 + 4;
     const uint8_t *mcol = a.mask + ic_t;
     uint32_t m_cur = __ldg(mcol + (size_t)clampi(rs, 0, ny - 1) * g.pitch);
     uint32_t m_nxt = __ldg(mcol + (size_t)clampi(rs + 1, 0, ny - 1) * g.pitch);
-    // per-thread constants of the update phase
-    const int iu = i0 + t;                  // update column
+    const int iu = i0 + t;
     const bool col_ok = (t < W) && (iu < nx);
     const bool edge_x = (iu == 0 || iu == nx - 1);
-    const int tx = min(t, W);               // x-face owner column (clamped)
-    const int cy = min(t, W - 1) + 2;       // y-face / update column in the staged row
+    const int tx = min(t, W);
+    const int cy = min(t, W - 1) + 2;
     float *outp = a.out + iu;
 
-    // rotating ring slots: raw (K) of rows r and r-2, parity of row r;
-    // primitive/mask ring (5) of rows r .. r-4; x-face ring (3) of rows r, r-2
-    int kr = 0, ku = K - 2, par = 0;
+    int kr = base % K, par = (base / K) & 1, ku = (base + K - 2) % K;
     int p0 = 0, p1 = PR - 1, p2 = PR - 2, p3 = PR - 3;
     int x0 = 0, x2 = XR - 2;
+    bool ok_all = true;
 
     for (int q = 0; q < nrows; q++) {
         const int r = rs + q;
@@ -198,13 +196,12 @@ __global__ void __launch_bounds__(NT) k_stage(const __grid_constant__ CUtensorMa
         m_cur = m_nxt;
         m_nxt = m_pf;
         if (__syncthreads_or(!ok)) {
-            aborted = true;
+            ok_all = false;
             break;
         }
         // ---- phase 2: x-face of row r owned by cell i0-1+t (t in [0, W]) and
-        // the y-face between rows r-2 and r-1 at column i0+t (t < W).  Both are
-        // evaluated by every thread (operands clamped in range) so the two
-        // independent Riemann problems interleave; only needed ones are stored.
+        // the y-face between rows r-2 and r-1 at column i0+t (t < W), both
+        // evaluated by every thread so the two Riemann problems interleave.
         {
             const float4 *Pr = P + p0 * NT;
             const uint32_t mbx = M[p0 * NT + tx + 1];
@@ -286,7 +283,6 @@ __global__ void __launch_bounds__(NT) k_stage(const __grid_constant__ CUtensorMa
 #pragma unroll
             for (int k = 0; k < 5; k++) dst[k * g.plane] = Un[k];
         }
-        // rotate ring slots to the next row
         kr = ring_next<K>(kr);
         par ^= (kr == 0) ? 1 : 0;
         ku = ring_next<K>(ku);
@@ -297,15 +293,39 @@ __global__ void __launch_bounds__(NT) k_stage(const __grid_constant__ CUtensorMa
         x0 = ring_next<XR>(x0);
         x2 = ring_next<XR>(x2);
     }
-    if (aborted) {
+    if (!ok_all) {
         if (t == 0) {
             record_error(a.sc, kErrTimeout);
-            // drain loads still in flight before the CTA's shared memory is released
-            for (int q = 0; q < issued; q++) mbar_wait_bounded(&bars[q % K], (uint32_t)((q / K) & 1), 20000000LL);
+            // drain loads still in flight before the shared memory is released
+            for (int q = 0; q < issued; q++)
+                mbar_wait_bounded(&bars[(base + q) % K], (uint32_t)(((base + q) / K) & 1), 20000000LL);
         }
-        return;
+        return false;
     }
-    if (a.cfl) block_max2_publish<NT>(lmax_speed, 0.0f, a.sc->red);
+    rp.base = base + nrows;
+    return true;
+}
+
+template <int NT, int K, int STAGE, int SCHEME, int LIM>
+__global__ void __launch_bounds__(NT) k_stage(const __grid_constant__ CUtensorMap tm_in,
+                                              const __grid_constant__ CUtensorMap tm_blend, const StepArgs a) {
+    using L = StageLayout<NT, K, STAGE>;
+    static_assert(L::total <= 227 * 1024, "shared memory");
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char *smem = aligned_smem(smem_raw);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bar_off);
+    if (threadIdx.x == 0) {
+        prefetch_tensormap(&tm_in);
+        if (STAGE == 2) prefetch_tensormap(&tm_blend);
+        for (int k = 0; k < K; k++) mbar_init(&bars[k], 1);
+        fence_barrier_init();
+    }
+    RingPos rp{0};
+    float lmax = 0.0f;
+    if (!stage_tile<NT, K, STAGE, SCHEME, LIM>(&tm_in, &tm_blend, a, blockIdx.x * L::W, blockIdx.y * a.rows_per_cta,
+                                               smem, rp, lmax))
+        return;
+    if (a.cfl) block_max2_publish<NT>(lmax, 0.0f, a.sc->red);
 }
 
 template <int NT, int K>
@@ -329,17 +349,16 @@ struct ViscLayout {
     static constexpr uint32_t tx_bytes = 5 * BW * 4;
 };
 
-// Viscous half step (fusedViscousDiffusionKernel, src/solver.cu:2251-2511),
-// out of place, marching like k_stage.  Primitives (u, v, T) of the input on
-// NT columns, stress/heat flux on NT-2 columns, update on W = NT-4 columns.
+// Viscous half step on one tile (fusedViscousDiffusionKernel,
+// src/solver.cu:2251-2511), out of place: primitives (u, v, T) of the input
+// on NT columns, stress/heat flux on NT-2 columns, update on W = NT-4.
 template <int NT, int K>
-__global__ void __launch_bounds__(NT) k_viscous(const __grid_constant__ CUtensorMap tm_in, const StepArgs a) {
+__device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const StepArgs &a, int i0, int j0,
+                                             unsigned char *smem, RingPos &rp, float &lmax_speed, float &lmax_nu) {
     using L = ViscLayout<NT, K>;
     constexpr int W = L::W, PR = L::PR, TR = L::TR;
     static_assert(PR == 5 && TR == 3, "ring sizes");
     constexpr int AHEAD = K - 3;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    unsigned char *smem = aligned_smem(smem_raw);
     float *raw = reinterpret_cast<float *>(smem + L::raw_off);
     float4 *P = reinterpret_cast<float4 *>(smem + L::p_off);  // {u, v, T, -}
     float *Tq = reinterpret_cast<float *>(smem + L::t_off);   // {txx, tyy, txy, qx, qy}
@@ -349,12 +368,9 @@ __global__ void __launch_bounds__(NT) k_viscous(const __grid_constant__ CUtensor
     const GridDesc g = a.g;
     const int nx = g.nx, ny = g.ny;
     const int t = threadIdx.x;
-    const int i0 = blockIdx.x * W;
-    const int j0 = blockIdx.y * a.rows_per_cta;
     const int j1 = min(j0 + a.rows_per_cta, ny);
     const int rs = j0 - 2;
     const int nrows = (j1 + 1) - rs + 1;
-
     const float dt = a.sc->dt * a.dt_scale;
     ViscArgs va;
     va.inv_2dx = 0.5f / g.dx;
@@ -364,31 +380,28 @@ __global__ void __launch_bounds__(NT) k_viscous(const __grid_constant__ CUtensor
     va.prandtl = a.prandtl;
     va.ref_prandtl = a.ref_prandtl != 0;
 
-    if (t == 0) {
-        prefetch_tensormap(&tm_in);
-        for (int k = 0; k < K; k++) mbar_init(&bars[k], 1);
-        fence_barrier_init();
-    }
+    fence_proxy_async_smem();
     __syncthreads();
+    const int base = rp.base;
+    int islot = base % K;
     auto issue = [&](int q) {
-        const int slot = q % K;
         const int row = clampi(rs + q, 0, ny - 1);
-        mbar_arrive_expect_tx(&bars[slot], L::tx_bytes);
+        mbar_arrive_expect_tx(&bars[islot], L::tx_bytes);
 #pragma unroll
         for (int b = 0; b < L::NB; b++)
-            tma_load_3d(raw + (size_t)slot * L::SLOT + b * kBoxStride, &tm_in, &bars[slot], i0 - 4 + b * kBox, row, 0);
+            tma_load_3d(raw + (size_t)islot * L::SLOT + b * kBoxStride, tm_in, &bars[islot], i0 - 4 + b * kBox, row,
+                        0);
+        islot = ring_next<K>(islot);
     };
-    if (t == 0)
-        for (int q = 0; q < min(AHEAD, nrows); q++) issue(q);
     int issued = min(AHEAD, nrows);
-    bool aborted = false;
-    float lmax_speed = 0.0f, lmax_nu = 0.0f;
+    if (t == 0)
+        for (int q = 0; q < issued; q++) issue(q);
+
     const int ic_t = clampi(i0 - 2 + t, 0, nx - 1);
     const int rc_t = ic_t - i0 + 4;
     const uint8_t *mcol = a.mask + ic_t;
     uint32_t m_cur = __ldg(mcol + (size_t)clampi(rs, 0, ny - 1) * g.pitch);
     uint32_t m_nxt = __ldg(mcol + (size_t)clampi(rs + 1, 0, ny - 1) * g.pitch);
-    // stress column i0-1+t (t < NT-2) and update column i0+t (t < W)
     const int is = i0 - 1 + t;
     const bool stress_col_in = (t < NT - 2) && is >= 0 && is < nx;
     const int iu = i0 + t;
@@ -396,11 +409,10 @@ __global__ void __launch_bounds__(NT) k_viscous(const __grid_constant__ CUtensor
     const bool interior_x = iu > 0 && iu < nx - 1;
     float *outp = a.out + iu;
 
-    // rotating slots: raw ring (K) rows r, r-2; primitives (5) rows r..r-3;
-    // stress ring (3) rows r-1 (written), r-2, r-3
-    int kr = 0, ku = K - 2, par = 0;
+    int kr = base % K, par = (base / K) & 1, ku = (base + K - 2) % K;
     int p0 = 0, p1 = PR - 1, p2 = PR - 2, p3 = PR - 3;
     int s1 = 0, s2 = TR - 1, s3 = TR - 2;
+    bool ok_all = true;
 
     for (int q = 0; q < nrows; q++) {
         const int r = rs + q;
@@ -417,7 +429,7 @@ __global__ void __launch_bounds__(NT) k_viscous(const __grid_constant__ CUtensor
         m_cur = m_nxt;
         m_nxt = m_pf;
         if (__syncthreads_or(!ok)) {
-            aborted = true;
+            ok_all = false;
             break;
         }
         // ---- phase 2: stress and heat flux of row r-1 at column i0-1+t
@@ -448,8 +460,8 @@ __global__ void __launch_bounds__(NT) k_viscous(const __grid_constant__ CUtensor
         // ---- phase 3: viscous update of row r-2 at column i0+t
         const int urow = r - 2;
         if (urow >= j0 && urow < j1 && col_ok) {
-            const int c = t + 2;  // primitive column
-            const int tc = t + 1; // stress column
+            const int c = t + 2;   // primitive column
+            const int tc = t + 1;  // stress column
             const uint32_t mb = M[p2 * NT + c];
             const uint32_t ctype = mb_type(mb);
             const float *src = raw + (size_t)ku * L::SLOT;
@@ -505,14 +517,128 @@ __global__ void __launch_bounds__(NT) k_viscous(const __grid_constant__ CUtensor
         s2 = s1;
         s1 = ring_next<TR>(s1);
     }
-    if (aborted) {
+    if (!ok_all) {
         if (t == 0) {
             record_error(a.sc, kErrTimeout);
-            for (int q = 0; q < issued; q++) mbar_wait_bounded(&bars[q % K], (uint32_t)((q / K) & 1), 20000000LL);
+            for (int q = 0; q < issued; q++)
+                mbar_wait_bounded(&bars[(base + q) % K], (uint32_t)(((base + q) / K) & 1), 20000000LL);
         }
-        return;
+        return false;
     }
-    if (a.cfl) block_max2_publish<NT>(lmax_speed, lmax_nu, a.sc->red);
+    rp.base = base + nrows;
+    return true;
+}
+
+template <int NT, int K>
+__global__ void __launch_bounds__(NT) k_viscous(const __grid_constant__ CUtensorMap tm_in, const StepArgs a) {
+    using L = ViscLayout<NT, K>;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char *smem = aligned_smem(smem_raw);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bar_off);
+    if (threadIdx.x == 0) {
+        prefetch_tensormap(&tm_in);
+        for (int k = 0; k < K; k++) mbar_init(&bars[k], 1);
+        fence_barrier_init();
+    }
+    RingPos rp{0};
+    float ls = 0.0f, ln = 0.0f;
+    if (!viscous_tile<NT, K>(&tm_in, a, blockIdx.x * L::W, blockIdx.y * a.rows_per_cta, smem, rp, ls, ln)) return;
+    if (a.cfl) block_max2_publish<NT>(ls, ln, a.sc->red);
+}
+
+// --------------------------------------------------------- batched launches
+// One persistent launch advances one stage of every instance of a batch:
+// CTAs walk a static tile list (instance, strip, row band); per-instance
+// descriptors give buffers, tensor maps, parameters and device scalars.  The
+// buffer that holds U^n alternates per step; each instance keeps its own
+// parity in its device scalars (flipped by its ghost-pass finalize).
+__device__ __forceinline__ int role_buf(const BatchInst &I, int role) {
+    const int parity = (int)I.sc->parity;
+    if (role == ROLE_N) return parity ? 2 : 0;
+    if (role == ROLE_X) return parity ? 0 : 2;
+    return role == ROLE_S ? 1 : 3;
+}
+
+__device__ __forceinline__ StepArgs batch_args(const BatchInst &I, int out_role, int apply_bc, int cfl, float dts,
+                                               int rows) {
+    StepArgs a;
+    a.g = I.g;
+    a.out = I.buf[role_buf(I, out_role)];
+    a.mask = I.mask;
+    a.sc = I.sc;
+    a.fs = I.fs;
+    a.wall = I.wall;
+    a.prandtl = I.prandtl;
+    a.ref_prandtl = I.ref_prandtl;
+    a.rows_per_cta = rows;
+    a.apply_bc = apply_bc;
+    a.cfl = cfl;
+    a.dt_scale = dts;
+    return a;
+}
+
+template <int NT, int K, int STAGE, int SCHEME, int LIM>
+__global__ void __launch_bounds__(NT) k_stage_batch(const BatchInst *__restrict__ insts,
+                                                    const TileDesc *__restrict__ tiles, int ntiles, int rows) {
+    using L = StageLayout<NT, K, STAGE>;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char *smem = aligned_smem(smem_raw);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bar_off);
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < K; k++) mbar_init(&bars[k], 1);
+        fence_barrier_init();
+    }
+    RingPos rp{0};
+    for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
+        const TileDesc td = tiles[ti];
+        const BatchInst &I = insts[td.inst];
+        const bool visc = I.viscous != 0;
+        int in_role, blend_role, out_role, bc, cfl;
+        if (STAGE == 1) {
+            in_role = visc ? ROLE_D : ROLE_N;
+            blend_role = in_role;
+            out_role = ROLE_S;
+            bc = 1;
+            cfl = 0;
+        } else {
+            in_role = ROLE_S;
+            blend_role = visc ? ROLE_D : ROLE_N;
+            out_role = visc ? ROLE_D : ROLE_X;
+            bc = visc ? 0 : 1;
+            cfl = visc ? 0 : 1;
+        }
+        const StepArgs a = batch_args(I, out_role, bc, cfl, 1.0f, rows);
+        float lmax = 0.0f;
+        if (!stage_tile<NT, K, STAGE, SCHEME, LIM>(&I.tm_in[role_buf(I, in_role)], &I.tm_ctr[role_buf(I, blend_role)],
+                                                   a, td.i0, td.j0, smem, rp, lmax))
+            return;
+        if (cfl) block_max2_publish<NT>(lmax, 0.0f, I.sc->red);
+    }
+}
+
+template <int NT, int K>
+__global__ void __launch_bounds__(NT) k_viscous_batch(const BatchInst *__restrict__ insts,
+                                                      const TileDesc *__restrict__ tiles, int ntiles, int rows,
+                                                      int post) {
+    using L = ViscLayout<NT, K>;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char *smem = aligned_smem(smem_raw);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bar_off);
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < K; k++) mbar_init(&bars[k], 1);
+        fence_barrier_init();
+    }
+    RingPos rp{0};
+    for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
+        const TileDesc td = tiles[ti];
+        const BatchInst &I = insts[td.inst];
+        // pre: U^n -> U_d (no BC); post: U_b -> U^{n+1} with BC and CFL
+        const int in_role = post ? ROLE_D : ROLE_N;
+        const StepArgs a = batch_args(I, post ? ROLE_X : ROLE_D, post, post ? 2 : 0, 0.5f, rows);
+        float ls = 0.0f, ln = 0.0f;
+        if (!viscous_tile<NT, K>(&I.tm_in[role_buf(I, in_role)], a, td.i0, td.j0, smem, rp, ls, ln)) return;
+        if (post) block_max2_publish<NT>(ls, ln, I.sc->red);
+    }
 }
 
 // ------------------------------------------------------------- ghost pass
@@ -543,75 +669,125 @@ __device__ void finalize_cfl(const GhostArgs &a) {
     }
     red[0] = 0.0f;
     red[1] = 0.0f;
+    if (a.flip_parity) sc->parity ^= 1u;
     __threadfence();
     sc->counter = 0;
 }
 
 // Ghost cells (src/solver.cu:2045-2225) with phase-2 semantics: neighbours
 // are read from the phase-1 state A, except neighbours that are themselves
-// ghost cells, whose pre-call value comes from B1/B2.
-__global__ void __launch_bounds__(128) k_ghost(const GhostArgs a) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    float ls = 0.0f, ln = 0.0f;
-    if (k < a.n) {
-        const GhostInfo gi = a.list[k];
-        const long long plane = a.g.plane;
-        long long best = -1;
-        bool best_gh = false;
-        for (int m = 0; m < gi.count; m++) {
-            const int code = (gi.cand >> (4 * m)) & 0xF;
-            const int d = code & 7;
-            const bool gh = (code & 8) != 0;
-            int di, dj;
-            ghost_neighbour(d, di, dj);
-            const long long q = (long long)gi.pidx + di + (long long)dj * a.g.pitch;
-            const float rq = gh ? pre_bc(a, q, 0) : a.A[q];
-            if (rq >= MIN_DENSITY) {
-                best = q;
-                best_gh = gh;
-                break;
-            }
-        }
-        float out[5];
-        if (best < 0) {
-            const float e_inf = a.fs.p / (GAMMA - 1.0f);
-            out[0] = a.fs.rho;
-            out[1] = 0.0f;
-            out[2] = 0.0f;
-            out[3] = e_inf;
-            out[4] = e_inf;
-        } else {
-            float s[4];
-#pragma unroll
-            for (int f = 0; f < 4; f++) s[f] = best_gh ? pre_bc(a, best, f) : a.A[f * plane + best];
-            ghost_state(s[0], s[1], s[2], s[3], gi.gx, gi.gy, a.wall, out);
-        }
-#pragma unroll
-        for (int f = 0; f < 5; f++) a.A[f * plane + gi.pidx] = out[f];
-        if (a.cfl) {
-            float uu, vv, pp, TT;
-            prim_from_cons(out[0], out[1], out[2], out[3], out[4], uu, vv, pp, TT);
-            ls = wave_speed(uu, vv, pp, out[0]);
-            if (a.cfl == 2) {
-                float pu, pv, ppp, pT;
-                prim_from_cons(pre_bc(a, gi.pidx, 0), pre_bc(a, gi.pidx, 1), pre_bc(a, gi.pidx, 2),
-                               pre_bc(a, gi.pidx, 3), pre_bc(a, gi.pidx, 4), pu, pv, ppp, pT);
-                ln = sutherland_mu(pT) / (out[0] + 1e-10f);
-            }
+// ghost cells, whose pre-call value comes from B1/B2.  Handles table entries
+// [first, first + count) with this block's threads; returns the thread's CFL
+// contributions.
+__device__ __forceinline__ void ghost_chunk(const GhostArgs &a, int first, int count, float &ls, float &ln) {
+    const int k = first + (int)threadIdx.x;
+    if ((int)threadIdx.x >= count || k >= a.n) return;
+    const GhostInfo gi = a.list[k];
+    const long long plane = a.g.plane;
+    long long best = -1;
+    bool best_gh = false;
+    for (int m = 0; m < gi.count; m++) {
+        const int code = (gi.cand >> (4 * m)) & 0xF;
+        const int d = code & 7;
+        const bool gh = (code & 8) != 0;
+        int di, dj;
+        ghost_neighbour(d, di, dj);
+        const long long q = (long long)gi.pidx + di + (long long)dj * a.g.pitch;
+        const float rq = gh ? pre_bc(a, q, 0) : a.A[q];
+        if (rq >= MIN_DENSITY) {
+            best = q;
+            best_gh = gh;
+            break;
         }
     }
+    float out[5];
+    if (best < 0) {
+        const float e_inf = a.fs.p / (GAMMA - 1.0f);
+        out[0] = a.fs.rho;
+        out[1] = 0.0f;
+        out[2] = 0.0f;
+        out[3] = e_inf;
+        out[4] = e_inf;
+    } else {
+        float s[4];
+#pragma unroll
+        for (int f = 0; f < 4; f++) s[f] = best_gh ? pre_bc(a, best, f) : a.A[f * plane + best];
+        ghost_state(s[0], s[1], s[2], s[3], gi.gx, gi.gy, a.wall, out);
+    }
+#pragma unroll
+    for (int f = 0; f < 5; f++) a.A[f * plane + gi.pidx] = out[f];
+    if (a.cfl) {
+        float uu, vv, pp, TT;
+        prim_from_cons(out[0], out[1], out[2], out[3], out[4], uu, vv, pp, TT);
+        ls = wave_speed(uu, vv, pp, out[0]);
+        if (a.cfl == 2) {
+            float pu, pv, ppp, pT;
+            prim_from_cons(pre_bc(a, gi.pidx, 0), pre_bc(a, gi.pidx, 1), pre_bc(a, gi.pidx, 2), pre_bc(a, gi.pidx, 3),
+                           pre_bc(a, gi.pidx, 4), pu, pv, ppp, pT);
+            ln = sutherland_mu(pT) / (out[0] + 1e-10f);
+        }
+    }
+}
+
+// Reduce the block's CFL contributions and, for the last of `nblocks`
+// blocks of this solve, publish the step's maxima / next dt.
+__device__ __forceinline__ void ghost_publish(const GhostArgs &a, float ls, float ln, unsigned nblocks) {
     if (a.cfl) block_max2_publish<128>(ls, ln, a.sc->red);
     if (a.finalize) {
         __shared__ bool last;
         __threadfence();
         __syncthreads();
-        if (threadIdx.x == 0) last = (atomicAdd(&a.sc->counter, 1u) == gridDim.x - 1);
+        if (threadIdx.x == 0) last = (atomicAdd(&a.sc->counter, 1u) == nblocks - 1);
         __syncthreads();
         if (last && threadIdx.x == 0) {
             __threadfence();
             finalize_cfl(a);
         }
     }
+}
+
+__global__ void __launch_bounds__(128) k_ghost(const GhostArgs a) {
+    float ls = 0.0f, ln = 0.0f;
+    ghost_chunk(a, blockIdx.x * 128, 128, ls, ln);
+    ghost_publish(a, ls, ln, gridDim.x);
+}
+
+// Batched ghost pass: one block per (instance, chunk of <=128 ghost cells).
+// mode 1 = after stage 1, mode 2 = end of step (CFL, finalize, parity flip).
+__global__ void __launch_bounds__(128) k_ghost_batch(const BatchInst *__restrict__ insts,
+                                                    const GhostChunk *__restrict__ chunks, int mode) {
+    const GhostChunk ch = chunks[blockIdx.x];
+    const BatchInst &I = insts[ch.inst];
+    const bool visc = I.viscous != 0;
+    GhostArgs a{};
+    a.g = I.g;
+    a.list = I.ghosts;
+    a.n = I.n_ghost;
+    a.sc = I.sc;
+    a.fs = I.fs;
+    a.wall = I.wall;
+    a.recompute_dt = I.recompute_dt;
+    a.cfl_num = I.cfl_num;
+    a.cfl_visc = I.cfl_visc;
+    a.min_dx = I.min_dx;
+    a.viscous = I.viscous;
+    if (mode == 1) {
+        a.A = I.buf[role_buf(I, ROLE_S)];
+        a.B1 = I.buf[role_buf(I, visc ? ROLE_D : ROLE_N)];
+        a.B2 = nullptr;
+        a.cfl = 0;
+        a.finalize = 0;
+    } else {
+        a.A = I.buf[role_buf(I, ROLE_X)];
+        a.B1 = I.buf[role_buf(I, visc ? ROLE_D : ROLE_N)];
+        a.B2 = visc ? nullptr : I.buf[role_buf(I, ROLE_S)];
+        a.cfl = visc ? 2 : 1;
+        a.finalize = 1;
+        a.flip_parity = 1;
+    }
+    float ls = 0.0f, ln = 0.0f;
+    ghost_chunk(a, ch.first, ch.count, ls, ln);
+    ghost_publish(a, ls, ln, (unsigned)I.n_gchunks);
 }
 
 // Phase-1 boundary conditions in place (set-up path).
@@ -683,14 +859,26 @@ static cudaError_t visc_attr_t() {
                                 (int)ViscLayout<NT, K>::total);
 }
 
+template <int NT, int K, int STAGE, int SCHEME, int LIM>
+static cudaError_t stage_batch_attr_t() {
+    using L = StageLayout<NT, K, STAGE>;
+    return cudaFuncSetAttribute(k_stage_batch<NT, K, STAGE, SCHEME, LIM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)L::total);
+}
+
 template <int NT, int K>
 static cudaError_t prepare_t() {
     cudaError_t e = cudaSuccess, r;
-#define FVM_A(S, A, B) if ((r = stage_attr_t<NT, K, S, A, B>()) != cudaSuccess) e = r;
+#define FVM_A(S, A, B)                                                          \
+    if ((r = stage_attr_t<NT, K, S, A, B>()) != cudaSuccess) e = r;             \
+    if ((r = stage_batch_attr_t<NT, K, S, A, B>()) != cudaSuccess) e = r;
     FVM_A(1, 0, 0) FVM_A(1, 0, 1) FVM_A(1, 1, 0) FVM_A(1, 1, 1)
     FVM_A(2, 0, 0) FVM_A(2, 0, 1) FVM_A(2, 1, 0) FVM_A(2, 1, 1)
 #undef FVM_A
     if ((r = visc_attr_t<NT, K>()) != cudaSuccess) e = r;
+    if ((r = cudaFuncSetAttribute(k_viscous_batch<NT, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)ViscLayout<NT, K>::total)) != cudaSuccess)
+        e = r;
     return e;
 }
 
@@ -749,6 +937,74 @@ cudaError_t launch_viscous(const StageTune &tn, const CUtensorMap &tm_in, const 
     if (tn.nt == 256 && tn.ring == 6) return launch_viscous_t<256, 6>(tm_in, a, st);
     if (tn.nt == 256 && tn.ring == 8) return launch_viscous_t<256, 8>(tm_in, a, st);
     return cudaErrorInvalidValue;
+}
+
+// ---- batched launches: persistent grids sized by occupancy
+template <class KERN>
+static int persistent_grid(KERN kern, int threads, size_t smem, int ntiles) {
+    int per_sm = 0, sms = 0, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+    int g = std::max(1, per_sm) * std::max(1, sms);
+    return std::max(1, std::min(g, ntiles));
+}
+
+template <int NT, int K, int STAGE, int SCHEME, int LIM>
+static cudaError_t launch_stage_batch_t(const BatchInst *insts, const TileDesc *tiles, int ntiles, int rows,
+                                        cudaStream_t st) {
+    using L = StageLayout<NT, K, STAGE>;
+    auto kern = k_stage_batch<NT, K, STAGE, SCHEME, LIM>;
+    const int grid = persistent_grid(kern, NT, L::total, ntiles);
+    kern<<<grid, NT, L::total, st>>>(insts, tiles, ntiles, rows);
+    return cudaGetLastError();
+}
+
+template <int NT, int K, int STAGE>
+static cudaError_t launch_stage_batch_s(int scheme, int lim, const BatchInst *insts, const TileDesc *tiles,
+                                        int ntiles, int rows, cudaStream_t st) {
+    if (scheme == 0 && lim == 0) return launch_stage_batch_t<NT, K, STAGE, 0, 0>(insts, tiles, ntiles, rows, st);
+    if (scheme == 0 && lim == 1) return launch_stage_batch_t<NT, K, STAGE, 0, 1>(insts, tiles, ntiles, rows, st);
+    if (scheme == 1 && lim == 0) return launch_stage_batch_t<NT, K, STAGE, 1, 0>(insts, tiles, ntiles, rows, st);
+    return launch_stage_batch_t<NT, K, STAGE, 1, 1>(insts, tiles, ntiles, rows, st);
+}
+
+cudaError_t launch_stage_batch(int stage, int scheme, int limiter, const StageTune &tn, const BatchInst *insts,
+                               const TileDesc *tiles, int ntiles, cudaStream_t st) {
+    if (ntiles <= 0) return cudaSuccess;
+#define FVM_SB(NT, K)                                                                                         \
+    if (tn.nt == NT && tn.ring == K)                                                                          \
+        return stage == 1 ? launch_stage_batch_s<NT, K, 1>(scheme, limiter, insts, tiles, ntiles, tn.rows, st) \
+                          : launch_stage_batch_s<NT, K, 2>(scheme, limiter, insts, tiles, ntiles, tn.rows, st);
+    FVM_SB(128, 6) FVM_SB(128, 8) FVM_SB(256, 6) FVM_SB(256, 8)
+#undef FVM_SB
+    return cudaErrorInvalidValue;
+}
+
+template <int NT, int K>
+static cudaError_t launch_viscous_batch_t(const BatchInst *insts, const TileDesc *tiles, int ntiles, int rows,
+                                          int post, cudaStream_t st) {
+    auto kern = k_viscous_batch<NT, K>;
+    const int grid = persistent_grid(kern, NT, ViscLayout<NT, K>::total, ntiles);
+    kern<<<grid, NT, ViscLayout<NT, K>::total, st>>>(insts, tiles, ntiles, rows, post);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_viscous_batch(const StageTune &tn, const BatchInst *insts, const TileDesc *tiles, int ntiles,
+                                 int post, cudaStream_t st) {
+    if (ntiles <= 0) return cudaSuccess;
+    if (tn.nt == 128 && tn.ring == 6) return launch_viscous_batch_t<128, 6>(insts, tiles, ntiles, tn.rows, post, st);
+    if (tn.nt == 128 && tn.ring == 8) return launch_viscous_batch_t<128, 8>(insts, tiles, ntiles, tn.rows, post, st);
+    if (tn.nt == 256 && tn.ring == 6) return launch_viscous_batch_t<256, 6>(insts, tiles, ntiles, tn.rows, post, st);
+    if (tn.nt == 256 && tn.ring == 8) return launch_viscous_batch_t<256, 8>(insts, tiles, ntiles, tn.rows, post, st);
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_ghost_batch(const BatchInst *insts, const GhostChunk *chunks, int nchunks, int mode,
+                               cudaStream_t st) {
+    if (nchunks <= 0) return cudaSuccess;
+    k_ghost_batch<<<nchunks, 128, 0, st>>>(insts, chunks, mode);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_ghost(const GhostArgs &a, cudaStream_t st) {

@@ -28,7 +28,10 @@ EXPORTS = [
     "fvm_write_fields", "fvm_read_primitives", "fvm_field_to_device", "fvm_cell_types_to_device",
     "fvm_vector_arrows", "fvm_max_temperature", "fvm_max_mach", "fvm_memory_usage", "fvm_gpu_mem_info",
     "fvm_diagnostics", "fvm_shock_standoff", "fvm_set_kernel_timing", "fvm_kernel_times",
-    "fvm_launch_count", "fvm_autotune", "fvm_get_tune", "fvm_debug_stage1", "fvm_debug_ghost_table", "fvm_build_info",
+    "fvm_launch_count", "fvm_batch_create", "fvm_batch_destroy", "fvm_batch_set_stream", "fvm_batch_add",
+    "fvm_batch_remove", "fvm_batch_count", "fvm_batch_step", "fvm_batch_synchronize", "fvm_batch_instance",
+    "fvm_batch_read_fields", "fvm_batch_diagnostics", "fvm_batch_memory_usage", "fvm_batch_launch_count",
+    "fvm_batch_instance_bytes", "fvm_autotune", "fvm_get_tune", "fvm_debug_stage1", "fvm_debug_ghost_table", "fvm_build_info",
 ]
 
 
@@ -94,6 +97,21 @@ def load_library(path=None):
     lib.fvm_launch_count.argtypes = [vp, C.POINTER(C.c_longlong)]
     lib.fvm_debug_stage1.argtypes = [vp, f, i] + [vp] * 5
     lib.fvm_autotune.argtypes = [vp, Pp, i, fp]
+    lib.fvm_batch_create.argtypes = [C.POINTER(vp), C.POINTER(Ext)]
+    lib.fvm_batch_destroy.argtypes = [vp]
+    lib.fvm_batch_set_stream.argtypes = [vp, vp]
+    lib.fvm_batch_add.argtypes = [vp, Pp, C.POINTER(i)]
+    lib.fvm_batch_remove.argtypes = [vp, i]
+    lib.fvm_batch_count.argtypes = [vp, C.POINTER(i)]
+    lib.fvm_batch_step.argtypes = [vp, i]
+    lib.fvm_batch_synchronize.argtypes = [vp]
+    lib.fvm_batch_instance.argtypes = [vp, i, Pp]
+    lib.fvm_batch_read_fields.argtypes = [vp, i] + [vp] * 5
+    lib.fvm_batch_diagnostics.argtypes = [vp, i, C.POINTER(Diag)]
+    lib.fvm_batch_memory_usage.argtypes = [vp, C.POINTER(sz)]
+    lib.fvm_batch_launch_count.argtypes = [vp, C.POINTER(C.c_longlong)]
+    lib.fvm_batch_instance_bytes.argtypes = [i, i]
+    lib.fvm_batch_instance_bytes.restype = sz
     lib.fvm_get_tune.argtypes = [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i)]
     lib.fvm_debug_ghost_table.argtypes = [vp, vp, i, C.POINTER(i)]
     _lib = lib
@@ -286,6 +304,83 @@ class Solver:
         return v.value
 
 
+class Batch:
+    """Many independent solves advanced together (fvm_batch_* in the C ABI)."""
+
+    def __init__(self, ext=None):
+        self.lib = load_library()
+        h = C.c_void_p()
+        self.ext = ext if ext is not None else ext_default()
+        _check(self.lib.fvm_batch_create(C.byref(h), C.byref(self.ext)))
+        self.h = h
+        self.shapes = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.fvm_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_handle):
+        _check(self.lib.fvm_batch_set_stream(self.h, C.c_void_p(stream_handle) if stream_handle else None))
+
+    def add(self, params):
+        i = C.c_int()
+        _check(self.lib.fvm_batch_add(self.h, C.byref(params), C.byref(i)))
+        self.shapes[i.value] = (params.ny, params.nx)
+        return i.value
+
+    def remove(self, id_):
+        _check(self.lib.fvm_batch_remove(self.h, int(id_)))
+        self.shapes.pop(id_, None)
+
+    def count(self):
+        n = C.c_int()
+        _check(self.lib.fvm_batch_count(self.h, C.byref(n)))
+        return n.value
+
+    def step(self, n=1):
+        _check(self.lib.fvm_batch_step(self.h, int(n)))
+
+    def synchronize(self):
+        _check(self.lib.fvm_batch_synchronize(self.h))
+
+    def instance(self, id_):
+        p = SimParams()
+        _check(self.lib.fvm_batch_instance(self.h, int(id_), C.byref(p)))
+        return p
+
+    def fields(self, id_):
+        ny, nx = self.shapes[id_]
+        out = [np.empty(nx * ny, np.float32) for _ in range(5)]
+        _check(self.lib.fvm_batch_read_fields(self.h, int(id_), *[_p(a) for a in out]))
+        return np.stack([a.reshape(ny, nx) for a in out])
+
+    def diagnostics(self, id_):
+        d = Diag()
+        _check(self.lib.fvm_batch_diagnostics(self.h, int(id_), C.byref(d)))
+        return d
+
+    def memory_usage(self):
+        v = C.c_size_t()
+        _check(self.lib.fvm_batch_memory_usage(self.h, C.byref(v)))
+        return v.value
+
+    def launch_count(self):
+        v = C.c_longlong()
+        _check(self.lib.fvm_batch_launch_count(self.h, C.byref(v)))
+        return v.value
+
+
+def instance_bytes(nx, ny):
+    return load_library().fvm_batch_instance_bytes(int(nx), int(ny))
+
+
 def gpu_mem_info():
     lib = load_library()
     f, t = C.c_size_t(), C.c_size_t()
@@ -293,5 +388,5 @@ def gpu_mem_info():
     return f.value, t.value
 
 
-__all__ = ["Solver", "FvmError", "SimParams", "Ext", "Diag", "params_default", "compute_derived",
+__all__ = ["Solver", "Batch", "instance_bytes", "FvmError", "SimParams", "Ext", "Diag", "params_default", "compute_derived",
            "ext_default", "workload", "load_library", "gpu_mem_info", "EXPORTS", "LIB_PATH"]

@@ -169,3 +169,62 @@ def workload(name, nx=None, ny=None):
         p.ny = ny
     compute_derived(p)
     return p, e
+
+
+def _splitmix64(state):
+    """One step of splitmix64: returns (new_state, 64-bit output)."""
+    state = (state + 0x9E3779B97F4A7C15) & 0xFFFFFFFFFFFFFFFF
+    z = state
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & 0xFFFFFFFFFFFFFFFF
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & 0xFFFFFFFFFFFFFFFF
+    return state, z ^ (z >> 31)
+
+
+class SeededStream:
+    """Deterministic uniform numbers from splitmix64 (platform independent)."""
+
+    def __init__(self, seed):
+        self.s = int(seed) & 0xFFFFFFFFFFFFFFFF
+
+    def uniform(self, lo=0.0, hi=1.0):
+        self.s, z = _splitmix64(self.s)
+        return lo + (hi - lo) * ((z >> 11) * (1.0 / (1 << 53)))
+
+    def log_uniform(self, lo, hi):
+        return math.exp(self.uniform(math.log(lo), math.log(hi)))
+
+    def choice(self, seq):
+        return seq[min(int(self.uniform() * len(seq)), len(seq) - 1)]
+
+
+def uneven_instance(rng, sizes=(128, 256, 512, 1024), mach=(0.3, 6.0), re=(1e2, 1e5), p_viscous=0.5):
+    """One synthetic solve of the uneven-batch workload: nx drawn from `sizes`,
+    ny = nx/2, Mach log-uniform, Euler or Navier-Stokes (Re log-uniform on the
+    obstacle diameter), obstacle from the reference shapes 0-4 with size
+    0.03-0.1 of the domain height and a random rotation.  SI mapping as in
+    `workload`: freestream 300 K / 101325 Pa; L = 1 m for Euler, L from the
+    Reynolds number for Navier-Stokes.  Returns (SimParams, Ext)."""
+    p = params_default()
+    e = ext_default()
+    nx = int(rng.choice(list(sizes)))
+    p.nx, p.ny = nx, nx // 2
+    p.T_inf, p.p_inf = 300.0, 101325.0
+    p.mach = rng.log_uniform(*mach)
+    viscous = rng.uniform() < p_viscous
+    size = rng.uniform(0.03, 0.1)
+    p.obstacle_shape = int(rng.choice([SHAPE_CIRCLE, SHAPE_STAR, SHAPE_DIAMOND, SHAPE_CAPSULE, SHAPE_TRIANGLE]))
+    p.obstacle_rotation = rng.uniform(0.0, 2.0 * math.pi)
+    reynolds = rng.log_uniform(*re)
+    p.enable_viscosity = viscous
+    compute_derived(p)
+    if viscous:
+        L = reynolds * sutherland(300.0) / (p.rho_inf * p.u_inf * 2.0 * size)
+    else:
+        L = 1.0
+    p.domain_width, p.domain_height = 2.0 * L, 1.0 * L
+    p.obstacle_x, p.obstacle_r = 0.4 * L, size * L
+    p.cfl = 0.5
+    compute_derived(p)
+    e.ref_length = 2.0 * size * L
+    e.dt_policy = DT_RECOMPUTE
+    return p, e

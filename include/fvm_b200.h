@@ -231,6 +231,32 @@ int fvm_autotune(fvm_handle *h, const fvm_sim_params *p, int steps, float *best_
 /* The launch tuning in use. */
 int fvm_get_tune(fvm_handle *h, int *nt, int *ring, int *rows);
 
+/* ------------------------------------------------------------ batches
+ * Many independent solves (different grids, Mach numbers, obstacles, Euler
+ * or Navier-Stokes) advanced together: each batched step is one persistent
+ * launch per stage over a tile list spanning every instance, replayed as one
+ * CUDA graph.  Every instance keeps its own time step (the ext's dt policy;
+ * FVM_DT_RECOMPUTE gives each its own CFL dt).  No reference counterpart. */
+typedef struct fvm_batch fvm_batch;
+int fvm_batch_create(fvm_batch **out, const fvm_ext *ext);
+int fvm_batch_destroy(fvm_batch *b);
+int fvm_batch_set_stream(fvm_batch *b, void *stream);
+/* Allocate and reset one instance (as fvm_initialize); *id_out is its id. */
+int fvm_batch_add(fvm_batch *b, const fvm_sim_params *p, int *id_out);
+int fvm_batch_remove(fvm_batch *b, int id);
+int fvm_batch_count(fvm_batch *b, int *n);
+/* n batched steps (every instance advances n steps). */
+int fvm_batch_step(fvm_batch *b, int n);
+int fvm_batch_synchronize(fvm_batch *b);
+/* Instance parameters with its t_current, step and last dt. */
+int fvm_batch_instance(fvm_batch *b, int id, fvm_sim_params *p_out);
+int fvm_batch_read_fields(fvm_batch *b, int id, float *rho, float *rho_u, float *rho_v, float *E, float *rho_e);
+int fvm_batch_diagnostics(fvm_batch *b, int id, fvm_diag *out);
+int fvm_batch_memory_usage(fvm_batch *b, size_t *bytes);
+int fvm_batch_launch_count(fvm_batch *b, long long *count_out);
+/* Device bytes one instance of nx*ny holds (admission estimate). */
+size_t fvm_batch_instance_bytes(int nx, int ny);
+
 /* Count of kernels this library launched on the handle since creation. */
 int fvm_launch_count(fvm_handle *h, long long *count_out);
 

@@ -31,7 +31,7 @@ EXPORTS = [
     "fvm_launch_count", "fvm_batch_create", "fvm_batch_destroy", "fvm_batch_set_stream", "fvm_batch_add",
     "fvm_batch_remove", "fvm_batch_count", "fvm_batch_step", "fvm_batch_synchronize", "fvm_batch_instance",
     "fvm_batch_read_fields", "fvm_batch_diagnostics", "fvm_batch_memory_usage", "fvm_batch_launch_count",
-    "fvm_batch_instance_bytes", "fvm_autotune", "fvm_get_tune", "fvm_debug_stage1", "fvm_debug_ghost_table", "fvm_build_info",
+    "fvm_batch_instance_bytes", "fvm_state_max_noalloc", "fvm_autotune", "fvm_get_tune", "fvm_debug_stage1", "fvm_debug_ghost_table", "fvm_build_info",
 ]
 
 
@@ -112,6 +112,7 @@ def load_library(path=None):
     lib.fvm_batch_launch_count.argtypes = [vp, C.POINTER(C.c_longlong)]
     lib.fvm_batch_instance_bytes.argtypes = [i, i]
     lib.fvm_batch_instance_bytes.restype = sz
+    lib.fvm_state_max_noalloc.argtypes = [vp, i, i, sz, sz, i, fp, vp]
     lib.fvm_get_tune.argtypes = [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i)]
     lib.fvm_debug_ghost_table.argtypes = [vp, vp, i, C.POINTER(i)]
     _lib = lib

@@ -257,6 +257,26 @@ int fvm_batch_launch_count(fvm_batch *b, long long *count_out);
 /* Device bytes one instance of nx*ny holds (admission estimate). */
 size_t fvm_batch_instance_bytes(int nx, int ny);
 
+/* ------------------------------------------------------------ no allocation
+ * Maximum temperature (what = 0) or local Mach number (what = 1) of a state
+ * held in the caller's device memory: five float planes (rho, rho*u, rho*v,
+ * E, rho*e) of ny rows by nx cells, `pitch` floats between rows and `plane`
+ * floats between planes.  *out (host memory) receives the maximum; the call
+ * returns when it is there.  No counterpart in the reference, which only
+ * reduces its own solver state (getMaxTemperature, src/solver.cu:2835-2867).
+ *
+ * Allocates nothing, for callers that may not allocate device memory at the
+ * point of the call (memory committed up front to solve instances, no handle
+ * to create): the reduction scratch is a fixed array inside the library,
+ * enough for ny <= 16384 rows; a larger ny is rejected with FVM_ERR_INVALID
+ * before anything runs.  The first call on each device looks up that array's
+ * address (cudaGetSymbolAddress, which may load the library's device code):
+ * make that first call before any stream capture begins.  All calls on one
+ * device share the array, so calls must not overlap: do not call it from two
+ * host threads at once for the same device. */
+int fvm_state_max_noalloc(const float *state, int nx, int ny, size_t pitch, size_t plane, int what, float *out,
+                          void *stream);
+
 /* Count of kernels this library launched on the handle since creation. */
 int fvm_launch_count(fvm_handle *h, long long *count_out);
 

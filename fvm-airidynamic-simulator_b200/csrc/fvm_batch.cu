@@ -24,6 +24,7 @@ struct fvm_batch {
     StageTune tune{128, 6, 32};
     std::vector<fvm_handle *> slots;  // instance id -> handle (nullptr when free)
     std::vector<long long> steps;     // steps taken per instance
+    std::vector<fvm_handle *> parked; // retired instances kept for reuse at the same grid size
     // device descriptors of the active instances
     BatchInst *d_insts = nullptr;
     TileDesc *d_stage_tiles = nullptr, *d_visc_tiles = nullptr;
@@ -99,7 +100,6 @@ static int rebuild(fvm_batch *b) {
             }
         for (int c = 0; c < I.n_gchunks; c++) chunks.push_back(GhostChunk{inst, c * 128, 128, 0});
     }
-    // interleave tiles of different instances so CTAs start on all of them
     if (int r = ensure(&b->d_insts, &b->cap_insts, insts.size())) return r;
     if (int r = ensure(&b->d_stage_tiles, &b->cap_stage, stiles.size())) return r;
     if (int r = ensure(&b->d_visc_tiles, &b->cap_visc, vtiles.size())) return r;
@@ -187,6 +187,7 @@ extern "C" int fvm_batch_destroy(fvm_batch *b) {
     drop_graph(b);
     for (fvm_handle *h : b->slots)
         if (h) fvm_destroy(h);
+    for (fvm_handle *h : b->parked) fvm_destroy(h);
     cudaFree(b->d_insts);
     cudaFree(b->d_stage_tiles);
     cudaFree(b->d_visc_tiles);
@@ -219,11 +220,26 @@ extern "C" int fvm_batch_add(fvm_batch *b, const fvm_sim_params *p, int *id_out)
     CHECK_BATCH(b);
     if (!p || !id_out) return berr(FVM_ERR_INVALID, "null argument");
     fvm_handle *h = nullptr;
-    if (int r = fvm_create(&h)) return r;
-    fvm_set_stream(h, b->stream);
-    if (int r = fvm_initialize(h, p, &b->ext)) {
-        fvm_destroy(h);
-        return r;
+    // a retired instance of the same grid size keeps its buffers: reset it in place
+    for (size_t k = 0; k < b->parked.size(); k++) {
+        fvm_handle *c = b->parked[k];
+        if (c->g.nx == p->nx && c->g.ny == p->ny) {
+            b->parked.erase(b->parked.begin() + (long)k);
+            if (int r = fvm_reset(c, p)) {
+                fvm_destroy(c);
+                return r;
+            }
+            h = c;
+            break;
+        }
+    }
+    if (!h) {
+        if (int r = fvm_create(&h)) return r;
+        fvm_set_stream(h, b->stream);
+        if (int r = fvm_initialize(h, p, &b->ext)) {
+            fvm_destroy(h);
+            return r;
+        }
     }
     // the batch launches one kernel shape for every instance
     if (h->tune.nt != b->tune.nt || h->tune.ring != b->tune.ring || h->tune.rows != b->tune.rows) {
@@ -241,14 +257,18 @@ extern "C" int fvm_batch_add(fvm_batch *b, const fvm_sim_params *p, int *id_out)
             return r;
         }
     }
+    // device scalars of the fresh solve, written on the batch stream (which
+    // does not synchronise with the legacy default stream)
     DevScalars init;
-    BCK(cudaMemcpy(&init, h->sc, sizeof init, cudaMemcpyDeviceToHost));
+    BCK(cudaMemcpyAsync(&init, h->sc, sizeof init, cudaMemcpyDeviceToHost, b->stream));
+    BCK(cudaStreamSynchronize(b->stream));
     init.dt = dt;
     init.t = p->t_current;
     init.parity = 0;
     init.counter = 0;
     init.red[0] = init.red[1] = 0.0f;
-    BCK(cudaMemcpy(h->sc, &init, sizeof init, cudaMemcpyHostToDevice));
+    BCK(cudaMemcpyAsync(h->sc, &init, sizeof init, cudaMemcpyHostToDevice, b->stream));
+    BCK(cudaStreamSynchronize(b->stream));
     int id = -1;
     for (size_t k = 0; k < b->slots.size(); k++)
         if (!b->slots[k]) {
@@ -276,6 +296,43 @@ extern "C" int fvm_batch_remove(fvm_batch *b, int id) {
     b->slots[id] = nullptr;
     b->dirty = true;
     return FVM_OK;
+}
+
+extern "C" int fvm_batch_retire(fvm_batch *b, int id) {
+    CHECK_BATCH(b);
+    fvm_handle *h = inst_of(b, id);
+    if (!h) return berr(FVM_ERR_INVALID, "unknown instance id");
+    b->parked.push_back(h);
+    b->slots[id] = nullptr;
+    b->dirty = true;
+    return FVM_OK;
+}
+
+extern "C" int fvm_batch_trim(fvm_batch *b, size_t keep_bytes, size_t *parked_bytes_out) {
+    CHECK_BATCH(b);
+    auto held = [](fvm_handle *h) {
+        size_t x = 0;
+        fvm_memory_usage(h, &x);
+        return x;
+    };
+    size_t total = 0;
+    for (fvm_handle *h : b->parked) total += held(h);
+    if (total > keep_bytes) BCK(cudaStreamSynchronize(b->stream));
+    // oldest first
+    while (total > keep_bytes && !b->parked.empty()) {
+        fvm_handle *h = b->parked.front();
+        total -= held(h);
+        b->parked.erase(b->parked.begin());
+        fvm_destroy(h);
+    }
+    if (parked_bytes_out) *parked_bytes_out = total;
+    return FVM_OK;
+}
+
+bool fvm_internal_batch_has_parked(fvm_batch *b, int nx, int ny) {
+    for (fvm_handle *h : b->parked)
+        if (h->g.nx == nx && h->g.ny == ny) return true;
+    return false;
 }
 
 extern "C" int fvm_batch_count(fvm_batch *b, int *n) {

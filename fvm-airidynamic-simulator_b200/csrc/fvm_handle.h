@@ -66,3 +66,5 @@ struct fvm_handle {
 int fvm_internal_build_maps(fvm_handle *h);
 int fvm_internal_compute_dt(fvm_handle *h, const fvm_sim_params *p, float *dt);
 int fvm_internal_set_error(int code, const char *msg);
+// true when the batch holds a retired instance of this grid size (reused by fvm_batch_add)
+bool fvm_internal_batch_has_parked(fvm_batch *b, int nx, int ny);

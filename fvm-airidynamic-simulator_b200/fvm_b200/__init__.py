@@ -13,7 +13,7 @@ import os
 
 import numpy as np
 
-from .abi import (SimParams, Ext, Diag, KernelTime, STATUS, params_default, compute_derived,
+from .abi import (SimParams, Ext, Diag, KernelTime, Result, ServerStats, STATUS, params_default, compute_derived,
                   ext_default, workload)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -31,7 +31,9 @@ EXPORTS = [
     "fvm_launch_count", "fvm_batch_create", "fvm_batch_destroy", "fvm_batch_set_stream", "fvm_batch_add",
     "fvm_batch_remove", "fvm_batch_count", "fvm_batch_step", "fvm_batch_synchronize", "fvm_batch_instance",
     "fvm_batch_read_fields", "fvm_batch_diagnostics", "fvm_batch_memory_usage", "fvm_batch_launch_count",
-    "fvm_batch_instance_bytes", "fvm_state_max_noalloc", "fvm_autotune", "fvm_get_tune", "fvm_debug_stage1", "fvm_debug_ghost_table", "fvm_build_info",
+    "fvm_batch_instance_bytes", "fvm_batch_retire", "fvm_batch_trim", "fvm_server_create", "fvm_server_submit",
+    "fvm_server_poll", "fvm_server_wait", "fvm_server_drain", "fvm_server_get_stats", "fvm_server_destroy",
+    "fvm_state_max_noalloc", "fvm_autotune", "fvm_get_tune", "fvm_debug_stage1", "fvm_debug_ghost_table", "fvm_build_info",
 ]
 
 
@@ -113,6 +115,15 @@ def load_library(path=None):
     lib.fvm_batch_instance_bytes.argtypes = [i, i]
     lib.fvm_batch_instance_bytes.restype = sz
     lib.fvm_state_max_noalloc.argtypes = [vp, i, i, sz, sz, i, fp, vp]
+    lib.fvm_batch_retire.argtypes = [vp, i]
+    lib.fvm_batch_trim.argtypes = [vp, sz, C.POINTER(sz)]
+    lib.fvm_server_create.argtypes = [C.POINTER(vp), C.POINTER(Ext), sz, i, i]
+    lib.fvm_server_submit.argtypes = [vp, Pp, i, vp, vp, vp, vp, vp, C.POINTER(C.c_longlong)]
+    lib.fvm_server_poll.argtypes = [vp, C.POINTER(Result), i, C.POINTER(i)]
+    lib.fvm_server_wait.argtypes = [vp, C.c_longlong, C.c_double, C.POINTER(Result)]
+    lib.fvm_server_drain.argtypes = [vp, C.c_double]
+    lib.fvm_server_get_stats.argtypes = [vp, C.POINTER(ServerStats)]
+    lib.fvm_server_destroy.argtypes = [vp]
     lib.fvm_get_tune.argtypes = [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i)]
     lib.fvm_debug_ghost_table.argtypes = [vp, vp, i, C.POINTER(i)]
     _lib = lib
@@ -340,6 +351,17 @@ class Batch:
         _check(self.lib.fvm_batch_remove(self.h, int(id_)))
         self.shapes.pop(id_, None)
 
+    def retire(self, id_):
+        """Take an instance out but keep its memory for a later add of the same grid size."""
+        _check(self.lib.fvm_batch_retire(self.h, int(id_)))
+        self.shapes.pop(id_, None)
+
+    def trim(self, keep_bytes=0):
+        """Free retired instances until at most keep_bytes stay parked; returns the bytes parked."""
+        v = C.c_size_t()
+        _check(self.lib.fvm_batch_trim(self.h, int(keep_bytes), C.byref(v)))
+        return v.value
+
     def count(self):
         n = C.c_int()
         _check(self.lib.fvm_batch_count(self.h, C.byref(n)))
@@ -378,6 +400,72 @@ class Batch:
         return v.value
 
 
+class Server:
+    """Continuous-batching request loop (fvm_server_* in the C ABI).
+
+    submit() queues a solve and returns a ticket; the final state lands in
+    host arrays owned by this object, handed back by wait()/poll() with the
+    result record."""
+
+    def __init__(self, ext=None, budget_bytes=150 * 10**9, max_active=0, chunk_steps=64):
+        self.lib = load_library()
+        self.ext = ext if ext is not None else ext_default()
+        h = C.c_void_p()
+        _check(self.lib.fvm_server_create(C.byref(h), C.byref(self.ext), int(budget_bytes), int(max_active),
+                                          int(chunk_steps)))
+        self.h = h
+        self.outputs = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.fvm_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, params, steps, keep_fields=True):
+        """Queue a solve of `steps` steps; returns its ticket."""
+        t = C.c_longlong()
+        if keep_fields:
+            arrs = [np.empty((params.ny, params.nx), np.float32) for _ in range(5)]
+            ptrs = [_p(a) for a in arrs]
+        else:
+            arrs, ptrs = None, [None] * 5
+        _check(self.lib.fvm_server_submit(self.h, C.byref(params), int(steps), *ptrs, C.byref(t)))
+        self.outputs[t.value] = arrs
+        return t.value
+
+    def _collect(self, r):
+        arrs = self.outputs.pop(r.ticket, None)
+        fields = np.stack(arrs) if arrs is not None and r.status == 0 else None
+        return r, fields
+
+    def wait(self, ticket, timeout_s=-1.0):
+        """(Result, fields or None) of one request."""
+        r = Result()
+        _check(self.lib.fvm_server_wait(self.h, int(ticket), float(timeout_s), C.byref(r)))
+        return self._collect(r)
+
+    def poll(self, cap=256):
+        """Finished requests not yet collected: list of (Result, fields or None)."""
+        buf = (Result * cap)()
+        n = C.c_int()
+        _check(self.lib.fvm_server_poll(self.h, buf, int(cap), C.byref(n)))
+        return [self._collect(Result.from_buffer_copy(buf[k])) for k in range(n.value)]
+
+    def drain(self, timeout_s=-1.0):
+        _check(self.lib.fvm_server_drain(self.h, float(timeout_s)))
+
+    def stats(self):
+        st = ServerStats()
+        _check(self.lib.fvm_server_get_stats(self.h, C.byref(st)))
+        return st
+
+
 def instance_bytes(nx, ny):
     return load_library().fvm_batch_instance_bytes(int(nx), int(ny))
 
@@ -389,5 +477,5 @@ def gpu_mem_info():
     return f.value, t.value
 
 
-__all__ = ["Solver", "Batch", "instance_bytes", "FvmError", "SimParams", "Ext", "Diag", "params_default", "compute_derived",
+__all__ = ["Solver", "Batch", "Server", "instance_bytes", "FvmError", "SimParams", "Ext", "Diag", "params_default", "compute_derived",
            "ext_default", "workload", "load_library", "gpu_mem_info", "EXPORTS", "LIB_PATH"]

@@ -63,6 +63,22 @@ class Diag(C.Structure):
         "wall_heat", "wall_heat_max")] + [("reserved", C.c_double * 6)]
 
 
+class Result(C.Structure):
+    """fvm_result: the outcome of one served request."""
+    _fields_ = [("ticket", C.c_longlong), ("status", C.c_int), ("steps", C.c_int), ("nx", C.c_int), ("ny", C.c_int),
+                ("t_final", C.c_float), ("dt_last", C.c_float), ("submit_s", C.c_double), ("admit_s", C.c_double),
+                ("done_s", C.c_double), ("diag", Diag)]
+
+
+class ServerStats(C.Structure):
+    """fvm_server_stats."""
+    _fields_ = [("submitted", C.c_longlong), ("completed", C.c_longlong), ("rejected", C.c_longlong),
+                ("batched_steps", C.c_longlong), ("active", C.c_int), ("pending", C.c_int),
+                ("budget_bytes", C.c_size_t), ("active_bytes", C.c_size_t), ("parked_bytes", C.c_size_t),
+                ("cell_updates", C.c_double), ("busy_s", C.c_double), ("step_ms_p50", C.c_double),
+                ("step_ms_p99", C.c_double), ("step_ms_mean", C.c_double), ("reserved", C.c_double * 4)]
+
+
 class KernelTime(C.Structure):
     _fields_ = [("name", C.c_char * 48), ("launches", C.c_longlong), ("total_ms", C.c_double)]
 

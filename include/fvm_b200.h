@@ -256,6 +256,64 @@ int fvm_batch_memory_usage(fvm_batch *b, size_t *bytes);
 int fvm_batch_launch_count(fvm_batch *b, long long *count_out);
 /* Device bytes one instance of nx*ny holds (admission estimate). */
 size_t fvm_batch_instance_bytes(int nx, int ny);
+/* Take an instance out of the batch but keep its device memory: a later
+ * fvm_batch_add of the same grid size resets it in place instead of
+ * allocating.  fvm_batch_remove frees the memory instead. */
+int fvm_batch_retire(fvm_batch *b, int id);
+/* Free retired instances (oldest first) until at most keep_bytes remain
+ * parked; *parked_bytes_out (may be NULL) receives what stays parked. */
+int fvm_batch_trim(fvm_batch *b, size_t keep_bytes, size_t *parked_bytes_out);
+
+/* ------------------------------------------------------------ serving
+ * A request loop over one batch (continuous batching).  Solve requests are
+ * submitted from any host thread and queue in arrival order; a worker thread
+ * admits them into the batch as instance slots and the device-memory budget
+ * allow (first come first served; a request larger than the whole budget is
+ * rejected with FVM_ERR_BUDGET), advances all admitted solves together in
+ * chunks of batched steps, and retires each one after its requested steps:
+ * its final state goes to the caller's host arrays (if given), its
+ * diagnostics into the result.  Each request's result equals the same solve
+ * run alone.  No reference counterpart. */
+typedef struct fvm_server fvm_server;
+typedef struct {
+    long long ticket;
+    int status;        /* FVM_OK, FVM_ERR_BUDGET, FVM_ERR_NONFINITE or the error that ended it */
+    int steps;         /* steps taken */
+    int nx, ny;
+    float t_final;     /* simulated time after the last step */
+    float dt_last;     /* time step of the last step */
+    double submit_s, admit_s, done_s; /* host clock, seconds since the server was created */
+    fvm_diag diag;     /* diagnostics of the final state */
+} fvm_result;
+typedef struct {
+    long long submitted, completed, rejected, batched_steps;
+    int active, pending;
+    size_t budget_bytes, active_bytes, parked_bytes;
+    double cell_updates;  /* cells x steps advanced */
+    double busy_s;        /* device time of the batched steps */
+    double step_ms_p50, step_ms_p99, step_ms_mean; /* device time per batched step */
+    double reserved[4];
+} fvm_server_stats;
+/* hbm_budget_bytes: device memory the admitted solves may hold (estimated by
+ * fvm_batch_instance_bytes); max_active: instance slots (0 = no limit);
+ * max_chunk_steps: most batched steps between admission checks (0 = 64).
+ * The worker uses the device current at creation. */
+int fvm_server_create(fvm_server **out, const fvm_ext *ext, size_t hbm_budget_bytes, int max_active,
+                      int max_chunk_steps);
+/* Queue a solve of `steps` steps from the freestream start of *p.  The five
+ * host arrays (nx*ny floats each, any may be NULL) receive the final state;
+ * they must stay valid until the result is collected. */
+int fvm_server_submit(fvm_server *s, const fvm_sim_params *p, int steps, float *rho, float *rho_u, float *rho_v,
+                      float *E, float *rho_e, long long *ticket_out);
+/* Collect up to cap finished results (completion order); *n_out receives how many. */
+int fvm_server_poll(fvm_server *s, fvm_result *out, int cap, int *n_out);
+/* Wait for one request's result (timeout_s < 0: no limit); FVM_ERR_TIMEOUT if it did not finish in time. */
+int fvm_server_wait(fvm_server *s, long long ticket, double timeout_s, fvm_result *out);
+/* Wait until every submitted request has finished (timeout_s < 0: no limit). */
+int fvm_server_drain(fvm_server *s, double timeout_s);
+int fvm_server_get_stats(fvm_server *s, fvm_server_stats *out);
+/* Stop the worker (requests not yet finished end with FVM_ERR_STATE) and free everything. */
+int fvm_server_destroy(fvm_server *s);
 
 /* ------------------------------------------------------------ no allocation
  * Maximum temperature (what = 0) or local Mach number (what = 1) of a state

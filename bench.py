@@ -40,7 +40,11 @@ WORKLOADS = {
     "ns_karman_re200": (2048, 1024),
     "euler_m3_circle": (512, 256),
     "reference_benchmark": (1024, 512),
+    # many-solve workloads (own code paths below)
+    "batched_uneven": (0, 0),
+    "serving": (0, 0),
 }
+BATCH_SEED, SERVE_SEED = 4, 5
 # Algorithmic HBM bytes per cell for each launch of the step (5 conserved
 # fields of 4 B, mask 1 B): input state read once, output written once,
 # blend partner read once.
@@ -163,6 +167,186 @@ def cpu_reference(params, ext, steps_budget_s=20.0, sample_nx=None, sample_ny=No
     return rate, threads, f"{nx}x{ny} grid of the same workload (1/{nx0 // nx} resolution), {n} FP64 steps in {el:.1f} s"
 
 
+def uneven_batch(n, seed=BATCH_SEED):
+    """The uneven batched workload: n seeded solves, nx in {128,256,512,1024},
+    ny = nx/2, Mach log-uniform 0.3-6, Euler or NS (Re log-uniform 1e2-1e5)
+    with p = 0.5, obstacle from the five reference shapes, size 0.03-0.1,
+    random rotation; each solve keeps its own CFL time step."""
+    rng = abi.SeededStream(seed)
+    return [abi.uneven_instance(rng) for _ in range(n)]
+
+
+def serving_requests(n, lam, seed=SERVE_SEED):
+    """Poisson arrivals at rate lam [1/s]: (arrival_s, params, steps); grid
+    nx in {256,512,1024,2048}, ny = nx/2, Mach log-uniform 0.3-8, Euler or NS
+    (Re log-uniform 1e2-1e5), obstacle as the uneven batch, steps uniform in
+    200-5000."""
+    import math
+    rng = abi.SeededStream(seed)
+    t, out = 0.0, []
+    for _ in range(n):
+        t += -math.log(1.0 - rng.uniform()) / lam
+        p, _ = abi.uneven_instance(rng, sizes=(256, 512, 1024, 2048), mach=(0.3, 8.0))
+        out.append((t, p, int(rng.uniform(200, 5001))))
+    return out
+
+
+def _events(torch):
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def solo_rate(torch, fvm_b200, p, ext, stream, steps):
+    """Device time of `steps` single-solve steps (graphs warmed for both parities)."""
+    s = fvm_b200.Solver(abi.SimParams.from_buffer_copy(p), ext)
+    s.set_stream(stream.cuda_stream)
+    with torch.cuda.stream(stream):
+        s.step(3)
+        s.step(3)
+        ev0, ev1 = _events(torch)
+        ev0.record(stream)
+        s.step(steps)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    s.close()
+    return ms
+
+
+def bench_batched(n_inst=256, steps=20, warmup=5, solo_steps=10):
+    """Batched step over the uneven workload vs the same solves one at a time."""
+    import torch
+    import fvm_b200
+    insts = uneven_batch(n_inst)
+    ext = insts[0][1]
+    cells = [p.nx * p.ny for p, _ in insts]
+    total = sum(cells)
+    stream = torch.cuda.Stream()
+    b = fvm_b200.Batch(ext)
+    b.set_stream(stream.cuda_stream)
+    ids = [b.add(p) for p, _ in insts]
+    with torch.cuda.stream(stream):
+        b.step(warmup)
+        torch.cuda.synchronize()
+        clocks = ClockSampler(torch.cuda.current_device())
+        clocks.start()
+        time.sleep(0.2)
+        n0 = b.launch_count()
+        ev0, ev1 = _events(torch)
+        ev0.record(stream)
+        b.step(steps)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1)
+        launches = b.launch_count() - n0
+        clk = clocks.stop()
+    finite = all(np.isfinite(b.diagnostics(i).mass) for i in ids)
+    # end to end through the API with host buffers: admit every solve (reusing
+    # the parked instances), `steps` batched steps, final states to host memory
+    outs = {i: [np.empty(p.nx * p.ny, np.float32) for _ in range(5)] for i, (p, _) in enumerate(insts)}
+    for i in ids:
+        b.retire(i)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ids2 = [b.add(p) for p, _ in insts]
+    b.step(steps)
+    for k, i in enumerate(ids2):
+        fvm_b200._check(b.lib.fvm_batch_read_fields(b.h, i, *[fvm_b200._p(a) for a in outs[k]]))
+    e2e_s = time.perf_counter() - t0
+    b.close()
+    # one solve at a time through the single-solve path (device time only)
+    solo_ms = 0.0
+    for p, e in insts:
+        solo_ms += solo_rate(torch, fvm_b200, p, e, stream, solo_steps)
+    rate = total * steps / (ms / 1e3)
+    solo = total * solo_steps / (solo_ms / 1e3)
+    visc = sum(c for c, (p, _) in zip(cells, insts) if p.enable_viscosity)
+    step_bytes = 102 * (total - visc) + 184 * visc
+    return {
+        "value": rate, "unit": "cell-updates/s", "ms_per_step": ms / steps, "instances": n_inst,
+        "cells": total, "steps": steps, "warmup": warmup,
+        "solves_per_s_at_500_steps": n_inst / (500 * ms / steps / 1e3),
+        "one_at_a_time": {"value": solo, "unit": "cell-updates/s",
+                          "sample": f"each of the {n_inst} solves alone, {solo_steps} steps, device time summed"},
+        "speedup_vs_one_at_a_time": rate / solo,
+        "step_gbs": step_bytes / (ms / steps / 1e3) / 1e9,
+        "e2e": {"value": total * steps / e2e_s, "unit": "cell-updates/s",
+                "h2d_bytes_per_step": n_inst * 112 / steps, "d2h_bytes_per_step": total * 20 / steps,
+                "includes": "admission of every solve (instance reuse), steps, final states to host"},
+        "gpu_launches": launches, "finite": bool(finite), "clocks": clk,
+    }
+
+
+def bench_serving(lams=(10.0, 100.0, 1000.0), n_req=24, chunk=64, budget=150 * 10**9, class_steps=20):
+    """Continuous-batching request loop on Poisson arrivals; the one-at-a-time
+    comparison is a FIFO single-solve queue on the same arrivals, each request
+    served at the measured single-solve rate of its grid/physics class."""
+    import torch
+    import fvm_b200
+    stream = torch.cuda.Stream()
+    ext = abi.ext_default()
+    ext.dt_policy = abi.DT_RECOMPUTE
+    # single-solve rate per (grid, viscous) class
+    class_rate = {}
+    rng = abi.SeededStream(SERVE_SEED + 1)
+    for nx in (256, 512, 1024, 2048):
+        for visc in (False, True):
+            while True:
+                p, _ = abi.uneven_instance(rng, sizes=(nx,), mach=(0.3, 8.0))
+                if bool(p.enable_viscosity) == visc:
+                    break
+            ms = solo_rate(torch, fvm_b200, p, ext, stream, class_steps)
+            class_rate[(nx, visc)] = p.nx * p.ny * class_steps / (ms / 1e3)
+    sweep = []
+    for lam in lams:
+        reqs = serving_requests(n_req, lam)
+        srv = fvm_b200.Server(ext, budget_bytes=budget, chunk_steps=chunk)
+        import threading
+        t_start = time.perf_counter()
+
+        def client():
+            for t, p, n in reqs:
+                d = t_start + t - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+                srv.submit(p, n, keep_fields=False)
+
+        th = threading.Thread(target=client)
+        th.start()
+        th.join()
+        srv.drain()
+        res = [r for r, _ in srv.poll(cap=n_req)]
+        st = srv.stats()
+        srv.close()
+        ok = [r for r in res if r.status == 0]
+        work = sum(r.nx * r.ny * r.steps for r in ok)
+        span = max(r.done_s for r in res) - min(r.submit_s for r in res)
+        lat = sorted(r.done_s - r.submit_s for r in ok)
+        # one at a time: FIFO queue, service = work / class rate
+        free_at, solo_lat = 0.0, []
+        for t, p, n in reqs:
+            start = max(t, free_at)
+            free_at = start + p.nx * p.ny * n / class_rate[(p.nx, bool(p.enable_viscosity))]
+            solo_lat.append(free_at - t)
+        solo_lat.sort()
+        solo_span = free_at - reqs[0][0]
+        solo_work = sum(p.nx * p.ny * n for _, p, n in reqs)
+        q = lambda v, f: v[min(len(v) - 1, int(round(f * (len(v) - 1))))] if v else None  # noqa: E731
+        sweep.append({
+            "lambda_per_s": lam, "requests": n_req, "completed_ok": len(ok), "failed": len(res) - len(ok),
+            "value": work / span, "unit": "cell-updates/s",
+            "completion_s_p50": q(lat, 0.5), "completion_s_p99": q(lat, 0.99),
+            "step_ms_p50": st.step_ms_p50, "step_ms_p99": st.step_ms_p99,
+            "device_busy_frac": st.busy_s / span,
+            "one_at_a_time": {"value": solo_work / solo_span, "unit": "cell-updates/s",
+                              "completion_s_p50": q(solo_lat, 0.5), "completion_s_p99": q(solo_lat, 0.99),
+                              "model": "FIFO single-solve queue on the same arrivals at measured per-class rates"},
+            "speedup_vs_one_at_a_time": (work / span) / (solo_work / solo_span),
+        })
+    return {"sweep": sweep, "class_rates": {f"{k[0]}x{k[0] // 2}{'_ns' if k[1] else '_euler'}": v
+                                            for k, v in class_rate.items()},
+            "budget_bytes": budget, "chunk_steps": chunk}
+
+
 def run_reference_arm(args, params, ext, ws, rank, dist):
     if rank != 0:
         return
@@ -190,6 +374,91 @@ def run_reference_arm(args, params, ext, ws, rank, dist):
     print(json.dumps(line), flush=True)
 
 
+def run_many_solves(args, ws, rank, local, dist):
+    """batched_uneven / serving: one line per run on rank 0 (other ranks run
+    replicas of the same work; weak scaling)."""
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        # the reference method on the host cores, one solve at a time, on a
+        # bounded sample of the same solves
+        if args.workload == "batched_uneven":
+            sample = [p for p, _ in uneven_batch(args.instances)]
+        else:
+            sample = [p for _, p, _ in serving_requests(args.requests, 100.0)]
+        budget = float(os.environ.get("FVM_CPU_BUDGET_S", "10"))
+        cu, secs, used, threads = 0.0, 0.0, 0, 1
+        from oracle.oracle import Oracle
+        e = abi.ext_default()
+        e.dt_policy = abi.DT_RECOMPUTE
+        threads = os.cpu_count() or 1
+        for p in sample:
+            o = Oracle(p, e, bits=64, threads=threads)
+            dt = o.compute_dt()
+            o.step(dt)
+            t0 = time.perf_counter()
+            n = 0
+            while n < 3 or (time.perf_counter() - t0) < budget / 8 and n < 20:
+                o.step(o.compute_dt())
+                n += 1
+            secs += time.perf_counter() - t0
+            cu += p.nx * p.ny * n
+            used += 1
+            if secs >= budget:
+                break
+        value = cu / secs
+        line = {"impl": "reference", "metric": "cell_updates_per_s", "value": value, "unit": "cell-updates/s",
+                "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded solves)", "config": {"workload": args.workload},
+                "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": threads, "kind": "port",
+                                 "sample": f"first {used} solves of the workload, one at a time, FP64"},
+                "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+    import torch
+    torch.cuda.set_device(local)
+    barrier(dist)
+    if args.workload == "batched_uneven":
+        r = bench_batched(n_inst=args.instances, steps=args.steps, warmup=args.warmup)
+        ms = max_over_ranks(r["ms_per_step"], dist)
+        value = r["cells"] * ws / (ms / 1e3)
+        hbm, peak_kind = load_peaks()
+        line = {
+            "metric": "cell_updates_per_s", "value": value, "unit": "cell-updates/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded solves)",
+            "config": {"workload": "batched_uneven", "instances": args.instances, "cells": r["cells"],
+                       "dt": "per-solve CFL", "l2": f"inputs > L2 ({r['cells'] * 20 / 1e6:.0f} MB per state set)"},
+            "roofline": {"bound": "hbm", "achieved": r["step_gbs"], "peak": hbm, "unit": "GB/s",
+                         "frac": r["step_gbs"] / hbm, "traffic": None, "kernel": "whole batched step",
+                         "algorithmic_bytes_per_cell": "102 (Euler) / 184 (NS)", "peak_kind": peak_kind},
+            "solves_per_s_at_500_steps": r["solves_per_s_at_500_steps"],
+            "one_at_a_time": r["one_at_a_time"], "speedup_vs_one_at_a_time": r["speedup_vs_one_at_a_time"],
+            "cpu_baseline": None, "e2e": r["e2e"], "gpu_launches": r["gpu_launches"], "clocks": r["clocks"],
+            "finite": r["finite"],
+        }
+    else:
+        lams = tuple(float(x) for x in args.lambdas.split(","))
+        r = bench_serving(lams=lams, n_req=args.requests)
+        top = r["sweep"][-1]
+        value = top["value"] * ws  # replicas of the same request stream
+        line = {
+            "metric": "cell_updates_per_s", "value": value, "unit": "cell-updates/s", "n_gpus": ws,
+            "steps": None, "warmup": None, "ms_per_step": top["step_ms_p50"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Poisson requests)",
+            "config": {"workload": "serving", "requests_per_rate": args.requests, "lambdas": list(lams),
+                       "budget_bytes": r["budget_bytes"], "chunk_steps": r["chunk_steps"]},
+            "latency": {"completion_s_p50": top["completion_s_p50"], "completion_s_p99": top["completion_s_p99"],
+                        "step_ms_p50": top["step_ms_p50"], "step_ms_p99": top["step_ms_p99"]},
+            "sweep": r["sweep"], "class_rates": r["class_rates"],
+            "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": None,
+                    "d2h_bytes_per_step": None, "includes": "submit from host to final diagnostics on host"},
+        }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -202,10 +471,20 @@ def main():
     ap.add_argument("--ny", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="skip the launch-shape autotuner")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="default workload only: skip the batched and serving summaries")
+    ap.add_argument("--instances", type=int, default=256, help="batched_uneven: number of solves")
+    ap.add_argument("--requests", type=int, default=96, help="serving: requests per arrival rate")
+    ap.add_argument("--lambdas", default="10,100,1000", help="serving: arrival rates [1/s]")
     args = ap.parse_args()
     assert args.warmup >= 3, "at least 3 warm-up steps"
 
     ws, rank, local, dist = dist_setup()
+    if args.workload in ("batched_uneven", "serving"):
+        run_many_solves(args, ws, rank, local, dist)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
     nx, ny = WORKLOADS[args.workload]
     nx, ny = args.nx or nx, args.ny or ny
     params, ext = abi.workload(args.workload, nx, ny)
@@ -295,6 +574,15 @@ def main():
         r, threads, sample = cpu_reference(params, ext, steps_budget_s=budget)
         cpu = {"value": r, "unit": "cell-updates/s", "cores": threads, "kind": "port", "sample": sample}
     step_gbs = value / ws * STEP_BYTES_FUSED / 1e9
+    s.close()
+    extras = {}
+    if rank == 0 and ws == 1 and not args.no_extras:
+        for name, fn in (("batched", lambda: bench_batched(n_inst=args.instances, steps=10, warmup=args.warmup)),
+                         ("serving", lambda: bench_serving(lams=(100.0,), n_req=16))):
+            try:
+                extras[name] = fn()
+            except Exception as exc:  # reported, never hides the main line
+                extras[name] = {"error": repr(exc)}
     if rank == 0:
         line = {
             "metric": "cell_updates_per_s", "value": value, "unit": "cell-updates/s", "n_gpus": ws,
@@ -316,9 +604,9 @@ def main():
                     "h2d_bytes_per_step": cells * 20 / args.steps, "d2h_bytes_per_step": cells * 20 / args.steps},
             "gpu_launches": launches,
             "clocks": clk,
+            **extras,
         }
         print(json.dumps(line), flush=True)
-    s.close()
     if dist is not None:
         dist.destroy_process_group()
 

@@ -574,6 +574,7 @@ def main():
         r, threads, sample = cpu_reference(params, ext, steps_budget_s=budget)
         cpu = {"value": r, "unit": "cell-updates/s", "cores": threads, "kind": "port", "sample": sample}
     step_gbs = value / ws * STEP_BYTES_FUSED / 1e9
+    tune = dict(zip(("threads", "ring", "rows_per_cta"), s.tune()))
     s.close()
     extras = {}
     if rank == 0 and ws == 1 and not args.no_extras:
@@ -593,7 +594,7 @@ def main():
                        "viscous": bool(params.enable_viscosity),
                        "flux": ["hllc", "ausm+"][ext.flux_scheme], "limiter": ["minmod", "van_leer"][ext.limiter],
                        "parallelism": f"replicas x{ws}", "l2": "inputs > L2 (670 MB per state), no flush",
-                       "tune": dict(zip(("threads", "ring", "rows_per_cta"), s.tune()))},
+                       "tune": tune},
             "hbm_gbs_per_gpu_at_102B": step_gbs,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": traffic, "kernel": dom_name,

@@ -625,6 +625,9 @@ static int check_device_error(fvm_handle *h) {
     CK(cudaStreamSynchronize(h->stream));
     if (h->h_sc->err & kErrTimeout)
         return set_err(FVM_ERR_TIMEOUT, "a bounded device wait expired (error word 0x%x)", h->h_sc->err);
+    if (h->h_sc->err & kErrSmemAlign)
+        return set_err(FVM_ERR_CUDA, "shared-memory staging area not 128-byte aligned; step skipped (error word 0x%x)",
+                       h->h_sc->err);
     return FVM_OK;
 }
 

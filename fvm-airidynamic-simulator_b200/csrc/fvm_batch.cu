@@ -408,6 +408,8 @@ extern "C" int fvm_batch_synchronize(fvm_batch *b) {
         DevScalars s;
         BCK(cudaMemcpy(&s, h->sc, sizeof s, cudaMemcpyDeviceToHost));
         if (s.err & kErrTimeout) return berr(FVM_ERR_TIMEOUT, "a bounded device wait expired in a batched step");
+        if (s.err & kErrSmemAlign)
+            return berr(FVM_ERR_CUDA, "shared-memory staging area not 128-byte aligned; batched step skipped");
     }
     return FVM_OK;
 }

@@ -68,10 +68,24 @@ __device__ __forceinline__ float ring_at(const float *slot_base, int f, int x) {
 }
 
 // Dynamic shared memory rounded up to a 128-byte boundary (the launch asks
-// for 128 extra bytes).
+// for 128 extra bytes).  The dynamic array follows the kernels' static shared
+// memory, so its start is only 16-byte aligned and the offset is computed at
+// run time.  The result is `p` plus that offset, never a pointer rebuilt from
+// an integer, so the compiler still knows it addresses shared memory and
+// emits shared loads/stores with 32-bit addressing instead of generic
+// accesses with 64-bit address arithmetic.
 __device__ __forceinline__ unsigned char *aligned_smem(unsigned char *p) {
-    const uintptr_t a = reinterpret_cast<uintptr_t>(p);
-    return reinterpret_cast<unsigned char *>((a + 127) & ~(uintptr_t)127);
+    const uint32_t a = smem_addr_opaque(p);
+    return p + (((a + 127u) & ~127u) - a);
+}
+
+// True (and the error recorded) when the staging area is not 128-byte
+// aligned; TMA destinations inside it would be misaligned.  Uniform over the
+// CTA, so every thread returns together.
+__device__ __forceinline__ bool smem_misaligned(const unsigned char *smem, DevScalars *sc) {
+    if ((smem_addr_opaque(smem) & 127u) == 0u) return false;
+    if (threadIdx.x == 0) atomicOr(&sc->err, kErrSmemAlign);
+    return true;
 }
 
 template <int NT, int K, int STAGE>
@@ -311,8 +325,9 @@ __global__ void __launch_bounds__(NT) k_stage(const __grid_constant__ CUtensorMa
                                               const __grid_constant__ CUtensorMap tm_blend, const StepArgs a) {
     using L = StageLayout<NT, K, STAGE>;
     static_assert(L::total <= 227 * 1024, "shared memory");
-    extern __shared__ __align__(128) unsigned char smem_raw[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned char *smem = aligned_smem(smem_raw);
+    if (smem_misaligned(smem, a.sc)) return;
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bar_off);
     if (threadIdx.x == 0) {
         prefetch_tensormap(&tm_in);
@@ -532,8 +547,9 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
 template <int NT, int K>
 __global__ void __launch_bounds__(NT) k_viscous(const __grid_constant__ CUtensorMap tm_in, const StepArgs a) {
     using L = ViscLayout<NT, K>;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned char *smem = aligned_smem(smem_raw);
+    if (smem_misaligned(smem, a.sc)) return;
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bar_off);
     if (threadIdx.x == 0) {
         prefetch_tensormap(&tm_in);
@@ -581,8 +597,9 @@ template <int NT, int K, int STAGE, int SCHEME, int LIM>
 __global__ void __launch_bounds__(NT) k_stage_batch(const BatchInst *__restrict__ insts,
                                                     const TileDesc *__restrict__ tiles, int ntiles, int rows) {
     using L = StageLayout<NT, K, STAGE>;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned char *smem = aligned_smem(smem_raw);
+    if (smem_misaligned(smem, insts[0].sc)) return;
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bar_off);
     if (threadIdx.x == 0) {
         for (int k = 0; k < K; k++) mbar_init(&bars[k], 1);
@@ -621,8 +638,9 @@ __global__ void __launch_bounds__(NT) k_viscous_batch(const BatchInst *__restric
                                                       const TileDesc *__restrict__ tiles, int ntiles, int rows,
                                                       int post) {
     using L = ViscLayout<NT, K>;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned char *smem = aligned_smem(smem_raw);
+    if (smem_misaligned(smem, insts[0].sc)) return;
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bar_off);
     if (threadIdx.x == 0) {
         for (int k = 0; k < K; k++) mbar_init(&bars[k], 1);

@@ -13,9 +13,22 @@ namespace fvm {
 constexpr long long kWaitCycles = 4000000000LL;  // ~2 s of SM clock per bounded wait
 constexpr uint32_t kErrTimeout = 1u;       // device error word bits
 constexpr uint32_t kErrNonFinite = 2u;
+constexpr uint32_t kErrSmemAlign = 4u;     // staging area not 128-byte aligned (kernel did nothing)
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-window address of p through an instruction the compiler does not
+// look into: no alignment it assumes for p (say, from an __align__ on an
+// extern __shared__ array) is folded into the result.
+__device__ __forceinline__ uint32_t smem_addr_opaque(const void *p) {
+    uint32_t a;
+    asm volatile(
+        "{\n\t.reg .u64 t;\n\tcvta.to.shared.u64 t, %1;\n\tcvt.u32.u64 %0, t;\n\t}"
+        : "=r"(a)
+        : "l"(p));
+    return a;
 }
 
 __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {

@@ -252,7 +252,7 @@ static StageTune pick_tune(const fvm_handle *h, int nx, int ny) {
     const char *env = getenv("FVM_TUNE");
     if (env) {
         int x = 0, y = 0, z = 0;
-        if (sscanf(env, "%d,%d,%d", &x, &y, &z) == 3 && (x == 128 || x == 256) && (y == 6 || y == 8) && z >= 4)
+        if (sscanf(env, "%d,%d,%d", &x, &y, &z) == 3 && (x == 128 || x == 256) && (y == 4 || y == 6) && z >= 4)
             return StageTune{x, y, z};
     }
     TuneKey k{nx, ny, h->prm.enable_viscosity ? 1 : 0, h->ext.flux_scheme, h->ext.limiter};
@@ -986,7 +986,7 @@ extern "C" int fvm_autotune(fvm_handle *h, const fvm_sim_params *p, int steps, f
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     int rc = FVM_OK;
-    const int nts[2] = {128, 256}, rings[2] = {6, 8}, rows[5] = {16, 32, 64, 128, 256};
+    const int nts[2] = {128, 256}, rings[2] = {4, 6}, rows[5] = {16, 32, 64, 128, 256};
     for (int a1 = 0; a1 < 2 && rc == FVM_OK; a1++)
         for (int a2 = 0; a2 < 2 && rc == FVM_OK; a2++)
             for (int a3 = 0; a3 < 5 && rc == FVM_OK; a3++) {

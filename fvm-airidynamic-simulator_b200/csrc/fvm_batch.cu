@@ -192,7 +192,7 @@ extern "C" int fvm_batch_create(fvm_batch **out, const fvm_ext *ext) {
     b->stream = b->own;
     if (const char *env = getenv("FVM_BATCH_TUNE")) {
         int x = 0, y = 0, z = 0;
-        if (sscanf(env, "%d,%d,%d", &x, &y, &z) == 3 && (x == 128 || x == 256) && (y == 6 || y == 8) && z >= 4) {
+        if (sscanf(env, "%d,%d,%d", &x, &y, &z) == 3 && (x == 128 || x == 256) && (y == 4 || y == 6) && z >= 4) {
             b->tune = StageTune{x, y, z};
             b->tune_fixed = true;
         }

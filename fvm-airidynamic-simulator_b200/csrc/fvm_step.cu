@@ -3,16 +3,13 @@
 //
 // Structure of a marching kernel.  A CTA of NT threads owns a strip of
 // W = NT-4 output columns and `rows` output rows.  It walks the strip from
-// bottom to top one row at a time.  Each incoming row (the 5 conserved planes
-// of the input state, columns [i0-4, i0+W+4)) is staged into a shared-memory
-// ring by one 3-D TMA load (x, y, field) signalled on an mbarrier, issued
-// ring-3 rows ahead.  Per row:
-//   phase 1  primitives of the incoming row r on NT columns (one per thread)
-//   phase 2  x-faces of row r (W+1 faces) and y-faces between rows r-2, r-1
-//   phase 3  update of row r-2 from the faces, RK blend, phase-1 boundary
-//            conditions, CFL contribution, coalesced store
-// so every face flux is computed exactly once per strip and each input cell
-// crosses HBM once (halo re-reads hit L2).  Domain-edge halos use the
+// bottom to top.  Each incoming row (the 5 conserved planes of the input
+// state, columns [i0-4, i0+W+4)) is staged into a shared-memory ring by a 3-D
+// TMA load (x, y, field) signalled on an mbarrier, issued ahead of use.  The
+// stage kernels advance two rows per step (primitives of the incoming rows,
+// their x-faces and two y-faces, update of the two rows two behind), the
+// viscous kernel one row per step, so every face flux is computed exactly
+// once per strip and each input cell crosses HBM once (halo re-reads hit L2).  Domain-edge halos use the
 // reference's clamp-to-edge semantics (src/solver.cu:1484-1488): rows by
 // clamping the TMA row coordinate, columns by clamping the shared-memory column.
 #include <algorithm>
@@ -93,26 +90,24 @@ struct StageLayout {
     static constexpr int W = NT - 4;   // output columns
     static constexpr int NB = (NT + 4 + kBox - 1) / kBox;  // TMA boxes per row
     static constexpr int BW = NB * kBox;  // staged columns [i0-4, i0-4+BW)
-    static constexpr int PR = 5;       // primitive / mask ring (rows)
-    static constexpr int XR = 3;       // x-face ring
-    static constexpr int YR = 2;       // y-face ring
-    static constexpr int SLOT = NB * kBoxStride;                       // floats per input slot
-    static constexpr int BSLOT = (int)(align128((size_t)5 * W * 4) / 4);  // floats per blend slot
+    static constexpr int KP = K / 2;   // input ring: K rows staged as K/2 row pairs
+    static constexpr int PP = 3;       // primitive / mask ring (row pairs)
+    static constexpr int XP = 1;       // x-face ring (row pairs)
+    static constexpr int SLOT = NB * kBoxStride;                       // floats per staged input row
+    static constexpr int BSLOT = (int)(align128((size_t)5 * W * 4) / 4);  // floats per staged blend row
     static constexpr size_t raw_off = 0;
     static constexpr size_t raw_bytes = (size_t)K * SLOT * 4;
     static constexpr size_t bl_off = raw_off + raw_bytes;
     static constexpr size_t bl_bytes = STAGE == 2 ? (size_t)K * BSLOT * 4 : 0;
     static constexpr size_t p_off = bl_off + bl_bytes;
-    static constexpr size_t p_bytes = (size_t)PR * NT * 16;
+    static constexpr size_t p_bytes = (size_t)PP * 2 * NT * 16;
     static constexpr size_t x_off = p_off + p_bytes;
-    static constexpr size_t x_bytes = (size_t)XR * 5 * NT * 4;
-    static constexpr size_t y_off = x_off + x_bytes;
-    static constexpr size_t y_bytes = (size_t)YR * 5 * NT * 4;
-    static constexpr size_t m_off = y_off + y_bytes;
-    static constexpr size_t m_bytes = (size_t)PR * NT;
+    static constexpr size_t x_bytes = (size_t)XP * 2 * 5 * NT * 4;
+    static constexpr size_t m_off = x_off + x_bytes;
+    static constexpr size_t m_bytes = (size_t)PP * 2 * NT;
     static constexpr size_t bar_off = (m_off + m_bytes + 15) & ~(size_t)15;
-    static constexpr size_t total = bar_off + K * 8 + 128;  // + alignment slack
-    static constexpr uint32_t tx_bytes = 5 * BW * 4 + (STAGE == 2 ? 5 * W * 4 : 0);
+    static constexpr size_t total = bar_off + KP * 8 + 128;  // + alignment slack
+    static constexpr uint32_t tx_bytes = 2 * (5 * BW * 4 + (STAGE == 2 ? 5 * W * 4 : 0));  // one row pair
 };
 
 // Slot bookkeeping of a row ring of N slots: rotating the indices of the
@@ -131,20 +126,30 @@ struct RingPos {
 
 // Inviscid SSP-RK2 stage on one tile (strip [i0, i0+W) x rows [j0, j1))
 // (computeFluxesKernel + updateKernel + [blend] + phase-1 BC,
-// src/solver.cu:1450-1876, :949-967, :1891-2042).  Returns false when a
-// bounded wait expired (error recorded; caller must stop).
+// src/solver.cu:1450-1876, :949-967, :1891-2042), marching two rows per step.
+// Per step q (incoming rows r = j0-2+2q and r+1):
+//   phase 1  primitives + masks of rows r, r+1 (one column per thread)
+//   -- barrier --
+//   phase 2  y-faces (r-2|r-1), (r-1|r) of column i0+t and the update of
+//            rows r-2, r-1 at column i0+t (x-faces of those rows from step q-1)
+//   -- barrier --
+//   phase 3  x-faces of rows r, r+1 (thread t: the face left of column i0+t)
+// The thread that computes a column's y-faces also updates that column, so
+// y-fluxes stay in registers (the face below row r-2 is carried from the
+// previous step).  After the second barrier nothing reads the previous row
+// pair's input slot or the primitives of pair q-2 again, which keeps the
+// rings at K/2 input pairs, 3 primitive pairs and 1 x-face pair.  Returns
+// false when a bounded wait expired (error recorded; caller must stop).
 template <int NT, int K, int STAGE, int SCHEME, int LIM>
 __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUtensorMap *tm_blend, const StepArgs &a,
                                            int i0, int j0, unsigned char *smem, RingPos &rp, float &lmax_speed) {
     using L = StageLayout<NT, K, STAGE>;
-    constexpr int W = L::W, PR = L::PR, XR = L::XR;
-    static_assert(PR == 5 && XR == 3, "ring sizes");
-    constexpr int AHEAD = K - 3;
+    constexpr int W = L::W, KP = L::KP;
+    static_assert(L::PP == 3 && L::XP == 1 && KP >= 2, "ring sizes");
     float *raw = reinterpret_cast<float *>(smem + L::raw_off);
     float *bl = reinterpret_cast<float *>(smem + L::bl_off);
     float4 *P = reinterpret_cast<float4 *>(smem + L::p_off);
     float *X = reinterpret_cast<float *>(smem + L::x_off);
-    float *Y = reinterpret_cast<float *>(smem + L::y_off);
     uint8_t *M = smem + L::m_off;
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bar_off);
 
@@ -153,34 +158,38 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
     const int t = threadIdx.x;
     const int j1 = min(j0 + a.rows_per_cta, ny);
     const int rs = j0 - 2;
-    const int nrows = (j1 + 1) - rs + 1;  // incoming rows rs .. j1+1
+    const int npairs = (j1 - j0 + 5) / 2;  // incoming rows rs .. j1+1 (one spare row when odd)
     const float dt = a.sc->dt * a.dt_scale;
     const UpdateArgs ua{dt, 1.0f / g.dx, 1.0f / g.dy};
 
     // slots of the previous tile are free once every thread is past its last read
     fence_proxy_async_smem();
     __syncthreads();
-    const int base = rp.base;
-    int islot = base % K;
+    const int base = rp.base;  // row pairs this CTA staged before this tile
+    int islot = base % KP;
     auto issue = [&](int q) {
-        const int row = clampi(rs + q, 0, ny - 1);
         mbar_arrive_expect_tx(&bars[islot], L::tx_bytes);
 #pragma unroll
-        for (int b = 0; b < L::NB; b++)
-            tma_load_3d(raw + (size_t)islot * L::SLOT + b * kBoxStride, tm_in, &bars[islot], i0 - 4 + b * kBox, row,
-                        0);
-        if (STAGE == 2) tma_load_3d(bl + (size_t)islot * L::BSLOT, tm_blend, &bars[islot], i0, row, 0);
-        islot = ring_next<K>(islot);
+        for (int h = 0; h < 2; h++) {
+            const int row = clampi(rs + 2 * q + h, 0, ny - 1);
+            float *dst = raw + (size_t)(islot * 2 + h) * L::SLOT;
+#pragma unroll
+            for (int b = 0; b < L::NB; b++)
+                tma_load_3d(dst + b * kBoxStride, tm_in, &bars[islot], i0 - 4 + b * kBox, row, 0);
+            if (STAGE == 2)
+                tma_load_3d(bl + (size_t)(islot * 2 + h) * L::BSLOT, tm_blend, &bars[islot], i0, row, 0);
+        }
+        islot = ring_next<KP>(islot);
     };
-    int issued = min(AHEAD, nrows);
+    int issued = min(KP, npairs);
     if (t == 0)
         for (int q = 0; q < issued; q++) issue(q);
 
     const int ic_t = clampi(i0 - 2 + t, 0, nx - 1);
     const int rc_t = ic_t - i0 + 4;
     const uint8_t *mcol = a.mask + ic_t;
-    uint32_t m_cur = __ldg(mcol + (size_t)clampi(rs, 0, ny - 1) * g.pitch);
-    uint32_t m_nxt = __ldg(mcol + (size_t)clampi(rs + 1, 0, ny - 1) * g.pitch);
+    uint32_t mA = __ldg(mcol + (size_t)clampi(rs, 0, ny - 1) * g.pitch);
+    uint32_t mB = __ldg(mcol + (size_t)clampi(rs + 1, 0, ny - 1) * g.pitch);
     const int iu = i0 + t;
     const bool col_ok = (t < W) && (iu < nx);
     const bool edge_x = (iu == 0 || iu == nx - 1);
@@ -188,135 +197,145 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
     const int cy = min(t, W - 1) + 2;
     float *outp = a.out + iu;
 
-    int kr = base % K, par = (base / K) & 1, ku = (base + K - 2) % K;
-    int p0 = 0, p1 = PR - 1, p2 = PR - 2, p3 = PR - 3;
-    int x0 = 0, x2 = XR - 2;
+    int kr = base % KP, par = (base / KP) & 1, ku = (base + KP - 1) % KP;
+    int pc0 = 0, pc1 = 4, pc2 = 2;  // P/M rows of row pairs q, q-1, q-2
+    float fyB[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};  // y-face below row r-2
     bool ok_all = true;
 
-    for (int q = 0; q < nrows; q++) {
-        const int r = rs + q;
-        const uint32_t m_pf = __ldg(mcol + (size_t)clampi(r + 2, 0, ny - 1) * g.pitch);
-        // ---- phase 1: primitives + mask of the incoming row
+    for (int q = 0; q < npairs; q++) {
+        const int r = rs + 2 * q;
+        const uint32_t nA = __ldg(mcol + (size_t)clampi(r + 2, 0, ny - 1) * g.pitch);
+        const uint32_t nB = __ldg(mcol + (size_t)clampi(r + 3, 0, ny - 1) * g.pitch);
+        // ---- phase 1: primitives + masks of rows r, r+1
         bool ok = mbar_wait_bounded(&bars[kr], (uint32_t)par);
         if (ok) {
-            const float *src = raw + (size_t)kr * L::SLOT;
-            float u, v, p, T;
-            const float rho = ring_at<L::NB>(src, 0, rc_t);
-            prim_from_cons(rho, ring_at<L::NB>(src, 1, rc_t), ring_at<L::NB>(src, 2, rc_t),
-                           ring_at<L::NB>(src, 3, rc_t), ring_at<L::NB>(src, 4, rc_t), u, v, p, T);
-            P[p0 * NT + t] = make_float4(rho, u, v, p);
-            M[p0 * NT + t] = (uint8_t)m_cur;
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const float *src = raw + (size_t)(kr * 2 + h) * L::SLOT;
+                float u, v, p, T;
+                const float rho = ring_at<L::NB>(src, 0, rc_t);
+                prim_from_cons(rho, ring_at<L::NB>(src, 1, rc_t), ring_at<L::NB>(src, 2, rc_t),
+                               ring_at<L::NB>(src, 3, rc_t), ring_at<L::NB>(src, 4, rc_t), u, v, p, T);
+                P[(pc0 + h) * NT + t] = make_float4(rho, u, v, p);
+                M[(pc0 + h) * NT + t] = (uint8_t)(h ? mB : mA);
+            }
         }
-        m_cur = m_nxt;
-        m_nxt = m_pf;
+        mA = nA;
+        mB = nB;
         if (__syncthreads_or(!ok)) {
             ok_all = false;
             break;
         }
-        // ---- phase 2: x-face of row r owned by cell i0-1+t (t in [0, W]) and
-        // the y-face between rows r-2 and r-1 at column i0+t (t < W), both
-        // evaluated by every thread so the two Riemann problems interleave.
+        // ---- phase 2: y-faces of column cy, then the update of rows r-2, r-1
+        const float4 c3 = P[(pc2 + 1) * NT + cy];  // column cy, row r-3
+        const float4 c2 = P[pc1 * NT + cy];        // r-2
+        const float4 c1 = P[(pc1 + 1) * NT + cy];  // r-1
+        const float4 c0 = P[pc0 * NT + cy];        // r
+        float fy0[5], fy1[5];
         {
-            const float4 *Pr = P + p0 * NT;
-            const uint32_t mbx = M[p0 * NT + tx + 1];
-            const float4 xm1 = Pr[tx], xa = Pr[tx + 1], xb = Pr[tx + 2], xp2 = Pr[tx + 3];
-            const float4 ym1 = P[p3 * NT + cy];
-            const float4 ya = P[p2 * NT + cy];
-            const float4 yb = P[p1 * NT + cy];
-            const float4 yp2 = Pr[cy];
-            const uint32_t mby = M[p2 * NT + cy];
-            float fx[5], fy[5];
-            face_flux<true, SCHEME, LIM>((mbx & MB_XV) != 0, (mbx & MB_XN) != 0, Prim{xm1.x, xm1.y, xm1.z, xm1.w},
-                                         Prim{xa.x, xa.y, xa.z, xa.w}, Prim{xb.x, xb.y, xb.z, xb.w},
-                                         Prim{xp2.x, xp2.y, xp2.z, xp2.w}, fx);
-            face_flux<false, SCHEME, LIM>((mby & MB_YV) != 0, (mby & MB_YN) != 0, Prim{ym1.x, ym1.y, ym1.z, ym1.w},
-                                          Prim{ya.x, ya.y, ya.z, ya.w}, Prim{yb.x, yb.y, yb.z, yb.w},
-                                          Prim{yp2.x, yp2.y, yp2.z, yp2.w}, fy);
-            if (r >= j0 && t <= W) {
-                float *Xs = X + x0 * 5 * NT + t;
+            const float4 cp = P[(pc0 + 1) * NT + cy];  // r+1
+            const uint32_t my0 = M[pc1 * NT + cy], my1 = M[(pc1 + 1) * NT + cy];
+            face_flux<false, SCHEME, LIM>((my0 & MB_YV) != 0, (my0 & MB_YN) != 0, Prim{c3.x, c3.y, c3.z, c3.w},
+                                          Prim{c2.x, c2.y, c2.z, c2.w}, Prim{c1.x, c1.y, c1.z, c1.w},
+                                          Prim{c0.x, c0.y, c0.z, c0.w}, fy0);
+            face_flux<false, SCHEME, LIM>((my1 & MB_YV) != 0, (my1 & MB_YN) != 0, Prim{c2.x, c2.y, c2.z, c2.w},
+                                          Prim{c1.x, c1.y, c1.z, c1.w}, Prim{c0.x, c0.y, c0.z, c0.w},
+                                          Prim{cp.x, cp.y, cp.z, cp.w}, fy1);
+        }
 #pragma unroll
-                for (int k = 0; k < 5; k++) Xs[k * NT] = fx[k];
-            }
-            if (r >= j0 + 1 && t < W) {
-                float *Ys = Y + ((r - 2) & 1) * 5 * NT + t;
+        for (int h = 0; h < 2; h++) {
+            const int urow = r - 2 + h;
+            if (urow >= j0 && urow < j1 && col_ok) {
+                const uint32_t mb = M[(pc1 + h) * NT + cy];
+                const float *src = raw + (size_t)(ku * 2 + h) * L::SLOT;
+                float Uc[5], Un[5];
 #pragma unroll
-                for (int k = 0; k < 5; k++) Ys[k * NT] = fy[k];
+                for (int k = 0; k < 5; k++) Uc[k] = ring_at<L::NB>(src, k, t + 4);
+                if (mb & MB_WALL) {
+#pragma unroll
+                    for (int k = 0; k < 5; k++) Un[k] = Uc[k];
+                } else {
+                    const float *Xs = X + h * 5 * NT + t;
+                    float fR[5], fL[5], fT[5], fB[5];
+#pragma unroll
+                    for (int k = 0; k < 5; k++) {
+                        fR[k] = Xs[k * NT + 1];
+                        fL[k] = Xs[k * NT];
+                        fT[k] = h ? fy1[k] : fy0[k];
+                        fB[k] = h ? fy0[k] : fyB[k];
+                    }
+                    const float4 pc = h ? c1 : c2;
+                    const float rxR = P[(pc1 + h) * NT + cy + 1].x, rxL = P[(pc1 + h) * NT + cy - 1].x;
+                    const float ryT = h ? c0.x : c1.x;
+                    const float ryB = h ? c2.x : c3.x;
+                    const bool edge_y = (urow == 0 || urow == ny - 1);
+                    update_cell(Uc, fR, fL, fT, fB, rxR, rxL, ryT, ryB, pc.w, edge_x, edge_y, !edge_x && !edge_y, ua,
+                                Un);
+                }
+                if (STAGE == 2) {
+                    const float *b = bl + (size_t)(ku * 2 + h) * L::BSLOT + t;
+#pragma unroll
+                    for (int k = 0; k < 5; k++) Un[k] = 0.5f * b[k * W] + 0.5f * Un[k];
+                }
+                const uint32_t ctype = mb_type(mb);
+                if (a.apply_bc) bc_pointwise(Un, ctype, iu, urow, nx, ny, a.fs);
+                if (a.cfl && ctype != CT_GHOST) {
+                    float uu, vv, pp, TT;
+                    prim_from_cons(Un[0], Un[1], Un[2], Un[3], Un[4], uu, vv, pp, TT);
+                    lmax_speed = fmaxf(lmax_speed, wave_speed(uu, vv, pp, Un[0]));
+                }
+                float *dst = outp + (size_t)urow * g.pitch;
+#pragma unroll
+                for (int k = 0; k < 5; k++) dst[k * g.plane] = Un[k];
             }
         }
+#pragma unroll
+        for (int k = 0; k < 5; k++) fyB[k] = fy1[k];
         fence_proxy_async_smem();
         __syncthreads();
-        // refill the ring slot freed by row q-3 (last read in phase 3 of q-1)
-        if (t == 0 && issued < nrows && issued <= q + AHEAD) {
+        // the input slot of pair q-1 is free now: stage pair q-1+KP into it
+        if (t == 0 && issued < npairs && issued <= q + KP - 1) {
             issue(issued);
             ++issued;
         }
-        // ---- phase 3: update row r-2
-        const int urow = r - 2;
-        if (urow >= j0 && urow < j1 && col_ok) {
-            const uint32_t mb = M[p2 * NT + cy];
-            const float *src = raw + (size_t)ku * L::SLOT;
-            float Uc[5], Un[5];
+        // ---- phase 3: x-faces of rows r, r+1 (read by the update in step q+1)
+        {
+            float fx0[5], fx1[5];
 #pragma unroll
-            for (int k = 0; k < 5; k++) Uc[k] = ring_at<L::NB>(src, k, t + 4);
-            if (mb & MB_WALL) {
-#pragma unroll
-                for (int k = 0; k < 5; k++) Un[k] = Uc[k];
-            } else {
-                const float *Xs = X + x2 * 5 * NT + t;
-                const float *Yt = Y + (urow & 1) * 5 * NT + t;
-                const float *Yb = Y + ((urow - 1) & 1) * 5 * NT + t;
-                float fR[5], fL[5], fT[5], fB[5];
+            for (int h = 0; h < 2; h++) {
+                const float4 *Pr = P + (pc0 + h) * NT;
+                const uint32_t mbx = M[(pc0 + h) * NT + tx + 1];
+                const float4 xm1 = Pr[tx], xa = Pr[tx + 1], xb = Pr[tx + 2], xp2 = Pr[tx + 3];
+                face_flux<true, SCHEME, LIM>((mbx & MB_XV) != 0, (mbx & MB_XN) != 0, Prim{xm1.x, xm1.y, xm1.z, xm1.w},
+                                             Prim{xa.x, xa.y, xa.z, xa.w}, Prim{xb.x, xb.y, xb.z, xb.w},
+                                             Prim{xp2.x, xp2.y, xp2.z, xp2.w}, h ? fx1 : fx0);
+            }
+            if (t <= W) {
+                float *Xs = X + t;
 #pragma unroll
                 for (int k = 0; k < 5; k++) {
-                    fR[k] = Xs[k * NT + 1];
-                    fL[k] = Xs[k * NT];
-                    fT[k] = Yt[k * NT];
-                    fB[k] = Yb[k * NT];
+                    Xs[k * NT] = fx0[k];
+                    Xs[(5 + k) * NT] = fx1[k];
                 }
-                const float4 pc = P[p2 * NT + cy];
-                const float rxR = P[p2 * NT + cy + 1].x, rxL = P[p2 * NT + cy - 1].x;
-                const float ryT = P[p1 * NT + cy].x;
-                const float ryB = P[p3 * NT + cy].x;
-                const bool edge_y = (urow == 0 || urow == ny - 1);
-                update_cell(Uc, fR, fL, fT, fB, rxR, rxL, ryT, ryB, pc.w, edge_x, edge_y, !edge_x && !edge_y, ua,
-                            Un);
             }
-            if (STAGE == 2) {
-                const float *b = bl + (size_t)ku * L::BSLOT + t;
-#pragma unroll
-                for (int k = 0; k < 5; k++) Un[k] = 0.5f * b[k * W] + 0.5f * Un[k];
-            }
-            const uint32_t ctype = mb_type(mb);
-            if (a.apply_bc) bc_pointwise(Un, ctype, iu, urow, nx, ny, a.fs);
-            if (a.cfl && ctype != CT_GHOST) {
-                float uu, vv, pp, TT;
-                prim_from_cons(Un[0], Un[1], Un[2], Un[3], Un[4], uu, vv, pp, TT);
-                lmax_speed = fmaxf(lmax_speed, wave_speed(uu, vv, pp, Un[0]));
-            }
-            float *dst = outp + (size_t)urow * g.pitch;
-#pragma unroll
-            for (int k = 0; k < 5; k++) dst[k * g.plane] = Un[k];
         }
-        kr = ring_next<K>(kr);
+        pc2 = pc1;
+        pc1 = pc0;
+        pc0 = (pc0 == 4) ? 0 : pc0 + 2;
+        kr = ring_next<KP>(kr);
         par ^= (kr == 0) ? 1 : 0;
-        ku = ring_next<K>(ku);
-        p3 = p2;
-        p2 = p1;
-        p1 = p0;
-        p0 = ring_next<PR>(p0);
-        x0 = ring_next<XR>(x0);
-        x2 = ring_next<XR>(x2);
+        ku = ring_next<KP>(ku);
     }
     if (!ok_all) {
         if (t == 0) {
             record_error(a.sc, kErrTimeout);
             // drain loads still in flight before the shared memory is released
             for (int q = 0; q < issued; q++)
-                mbar_wait_bounded(&bars[(base + q) % K], (uint32_t)(((base + q) / K) & 1), 20000000LL);
+                mbar_wait_bounded(&bars[(base + q) % KP], (uint32_t)(((base + q) / KP) & 1), 20000000LL);
         }
         return false;
     }
-    rp.base = base + nrows;
+    rp.base = base + npairs;
     return true;
 }
 
@@ -332,7 +351,7 @@ __global__ void __launch_bounds__(NT) k_stage(const __grid_constant__ CUtensorMa
     if (threadIdx.x == 0) {
         prefetch_tensormap(&tm_in);
         if (STAGE == 2) prefetch_tensormap(&tm_blend);
-        for (int k = 0; k < K; k++) mbar_init(&bars[k], 1);
+        for (int k = 0; k < L::KP; k++) mbar_init(&bars[k], 1);
         fence_barrier_init();
     }
     RingPos rp{0};
@@ -602,7 +621,7 @@ __global__ void __launch_bounds__(NT) k_stage_batch(const BatchInst *__restrict_
     if (smem_misaligned(smem, insts[0].sc)) return;
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bar_off);
     if (threadIdx.x == 0) {
-        for (int k = 0; k < K; k++) mbar_init(&bars[k], 1);
+        for (int k = 0; k < L::KP; k++) mbar_init(&bars[k], 1);
         fence_barrier_init();
     }
     RingPos rp{0};
@@ -849,15 +868,15 @@ size_t stage_smem_bytes(int stage, const StageTune &tn) {
 #define FVM_SZ(NT, K)                                                                              \
     if (tn.nt == NT && tn.ring == K)                                                               \
         return stage == 1 ? StageLayout<NT, K, 1>::total : StageLayout<NT, K, 2>::total;
-    FVM_SZ(128, 6) FVM_SZ(128, 8) FVM_SZ(256, 6) FVM_SZ(256, 8)
+    FVM_SZ(128, 4) FVM_SZ(128, 6) FVM_SZ(256, 4) FVM_SZ(256, 6)
 #undef FVM_SZ
     return 0;
 }
 size_t viscous_smem_bytes(const StageTune &tn) {
     if (tn.nt == 128 && tn.ring == 6) return ViscLayout<128, 6>::total;
-    if (tn.nt == 128 && tn.ring == 8) return ViscLayout<128, 8>::total;
+    if (tn.nt == 128 && tn.ring == 4) return ViscLayout<128, 4>::total;
     if (tn.nt == 256 && tn.ring == 6) return ViscLayout<256, 6>::total;
-    if (tn.nt == 256 && tn.ring == 8) return ViscLayout<256, 8>::total;
+    if (tn.nt == 256 && tn.ring == 4) return ViscLayout<256, 4>::total;
     return 0;
 }
 int stage_cols_per_cta(const StageTune &tn) { return tn.nt - 4; }
@@ -904,9 +923,9 @@ static cudaError_t prepare_t() {
 // once at set-up, outside any stream capture).
 cudaError_t prepare_step_kernels(const StageTune &tn) {
     if (tn.nt == 128 && tn.ring == 6) return prepare_t<128, 6>();
-    if (tn.nt == 128 && tn.ring == 8) return prepare_t<128, 8>();
+    if (tn.nt == 128 && tn.ring == 4) return prepare_t<128, 4>();
     if (tn.nt == 256 && tn.ring == 6) return prepare_t<256, 6>();
-    if (tn.nt == 256 && tn.ring == 8) return prepare_t<256, 8>();
+    if (tn.nt == 256 && tn.ring == 4) return prepare_t<256, 4>();
     return cudaErrorInvalidValue;
 }
 
@@ -935,7 +954,7 @@ cudaError_t launch_stage(int stage, int scheme, int limiter, const StageTune &tn
     if (tn.nt == NT && tn.ring == K)                                                                       \
         return stage == 1 ? launch_stage_s<NT, K, 1>(scheme, limiter, tn, tm_in, tm_blend, a, st)          \
                           : launch_stage_s<NT, K, 2>(scheme, limiter, tn, tm_in, tm_blend, a, st);
-    FVM_ST(128, 6) FVM_ST(128, 8) FVM_ST(256, 6) FVM_ST(256, 8)
+    FVM_ST(128, 4) FVM_ST(128, 6) FVM_ST(256, 4) FVM_ST(256, 6)
 #undef FVM_ST
     return cudaErrorInvalidValue;
 }
@@ -951,9 +970,9 @@ static cudaError_t launch_viscous_t(const CUtensorMap &tm_in, const StepArgs &a,
 
 cudaError_t launch_viscous(const StageTune &tn, const CUtensorMap &tm_in, const StepArgs &a, cudaStream_t st) {
     if (tn.nt == 128 && tn.ring == 6) return launch_viscous_t<128, 6>(tm_in, a, st);
-    if (tn.nt == 128 && tn.ring == 8) return launch_viscous_t<128, 8>(tm_in, a, st);
+    if (tn.nt == 128 && tn.ring == 4) return launch_viscous_t<128, 4>(tm_in, a, st);
     if (tn.nt == 256 && tn.ring == 6) return launch_viscous_t<256, 6>(tm_in, a, st);
-    if (tn.nt == 256 && tn.ring == 8) return launch_viscous_t<256, 8>(tm_in, a, st);
+    if (tn.nt == 256 && tn.ring == 4) return launch_viscous_t<256, 4>(tm_in, a, st);
     return cudaErrorInvalidValue;
 }
 
@@ -994,7 +1013,7 @@ cudaError_t launch_stage_batch(int stage, int scheme, int limiter, const StageTu
     if (tn.nt == NT && tn.ring == K)                                                                          \
         return stage == 1 ? launch_stage_batch_s<NT, K, 1>(scheme, limiter, insts, tiles, ntiles, tn.rows, st) \
                           : launch_stage_batch_s<NT, K, 2>(scheme, limiter, insts, tiles, ntiles, tn.rows, st);
-    FVM_SB(128, 6) FVM_SB(128, 8) FVM_SB(256, 6) FVM_SB(256, 8)
+    FVM_SB(128, 4) FVM_SB(128, 6) FVM_SB(256, 4) FVM_SB(256, 6)
 #undef FVM_SB
     return cudaErrorInvalidValue;
 }
@@ -1012,9 +1031,9 @@ cudaError_t launch_viscous_batch(const StageTune &tn, const BatchInst *insts, co
                                  int post, cudaStream_t st) {
     if (ntiles <= 0) return cudaSuccess;
     if (tn.nt == 128 && tn.ring == 6) return launch_viscous_batch_t<128, 6>(insts, tiles, ntiles, tn.rows, post, st);
-    if (tn.nt == 128 && tn.ring == 8) return launch_viscous_batch_t<128, 8>(insts, tiles, ntiles, tn.rows, post, st);
+    if (tn.nt == 128 && tn.ring == 4) return launch_viscous_batch_t<128, 4>(insts, tiles, ntiles, tn.rows, post, st);
     if (tn.nt == 256 && tn.ring == 6) return launch_viscous_batch_t<256, 6>(insts, tiles, ntiles, tn.rows, post, st);
-    if (tn.nt == 256 && tn.ring == 8) return launch_viscous_batch_t<256, 8>(insts, tiles, ntiles, tn.rows, post, st);
+    if (tn.nt == 256 && tn.ring == 4) return launch_viscous_batch_t<256, 4>(insts, tiles, ntiles, tn.rows, post, st);
     return cudaErrorInvalidValue;
 }
 

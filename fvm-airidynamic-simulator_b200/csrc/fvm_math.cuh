@@ -202,35 +202,38 @@ __device__ __forceinline__ void ausm_plus_flux(float rhoL, float unL, float utL,
     f[3] = a * rhoL * HL + b * rhoR * HR;
 }
 
-// One face of computeFluxesKernel (x: src/solver.cu:1502-1598, y: :1601-1682):
-// MUSCL reconstruction of (rho, u, v, p) from cells m1, a | b, p2, clamps,
-// Riemann flux and the upwinded rho_e flux.  `valid`: neither a nor b is a
-// wall; `first_order`: a wall at m1/p2 (density test is done here).
-// out = {mass, x-momentum, y-momentum, energy, rho_e}.
-template <bool XDIR, int SCHEME, int LIM>
-__device__ __forceinline__ void face_flux(bool valid, bool near_wall, const Prim &m1, const Prim &a, const Prim &b,
-                                          const Prim &p2, float out[5]) {
+// Limited slopes of cell c from its neighbours m and p along one direction,
+// in the face frame (rho, normal velocity, tangential velocity, p).
+template <bool XDIR, int LIM>
+__device__ __forceinline__ void cell_slopes(const Prim &m, const Prim &c, const Prim &p, float s[4]) {
+    s[0] = limited_slope<LIM>(m.rho, c.rho, p.rho);
+    s[1] = XDIR ? limited_slope<LIM>(m.u, c.u, p.u) : limited_slope<LIM>(m.v, c.v, p.v);
+    s[2] = XDIR ? limited_slope<LIM>(m.v, c.v, p.v) : limited_slope<LIM>(m.u, c.u, p.u);
+    s[3] = limited_slope<LIM>(m.p, c.p, p.p);
+}
+
+// One face of computeFluxesKernel (x: src/solver.cu:1502-1598, y: :1601-1682)
+// from the two cells a | b and their limited slopes sa, sb (cell_slopes):
+// MUSCL reconstruction of (rho, u, v, p), clamps, Riemann flux and the
+// upwinded rho_e flux.  `valid`: neither a nor b is a wall; `near_wall`:
+// first order (a wall at the outer stencil cells; the density test is done
+// here).  out = {mass, x-momentum, y-momentum, energy, rho_e}.
+template <bool XDIR, int SCHEME>
+__device__ __forceinline__ void face_flux_sl(bool valid, bool near_wall, const Prim &a, const float sa[4],
+                                             const Prim &b, const float sb[4], float out[5]) {
     if (valid) {
         bool lowDensity = (a.rho < LOW_DENSITY || b.rho < LOW_DENSITY);
         float order_mask = (near_wall || lowDensity) ? 0.0f : 1.0f;
-        const float am1 = XDIR ? m1.u : m1.v, aa = XDIR ? a.u : a.v, ab = XDIR ? b.u : b.v, ap2 = XDIR ? p2.u : p2.v;
-        const float tm1 = XDIR ? m1.v : m1.u, ta = XDIR ? a.v : a.u, tb = XDIR ? b.v : b.u, tp2 = XDIR ? p2.v : p2.u;
-        float slope_rho_L = limited_slope<LIM>(m1.rho, a.rho, b.rho);
-        float slope_un_L = limited_slope<LIM>(am1, aa, ab);
-        float slope_ut_L = limited_slope<LIM>(tm1, ta, tb);
-        float slope_p_L = limited_slope<LIM>(m1.p, a.p, b.p);
-        float rhoL = a.rho + 0.5f * slope_rho_L * order_mask;
-        float unL = aa + 0.5f * slope_un_L * order_mask;
-        float utL = ta + 0.5f * slope_ut_L * order_mask;
-        float pL = a.p + 0.5f * slope_p_L * order_mask;
-        float slope_rho_R = limited_slope<LIM>(a.rho, b.rho, p2.rho);
-        float slope_un_R = limited_slope<LIM>(aa, ab, ap2);
-        float slope_ut_R = limited_slope<LIM>(ta, tb, tp2);
-        float slope_p_R = limited_slope<LIM>(a.p, b.p, p2.p);
-        float rhoR = b.rho - 0.5f * slope_rho_R * order_mask;
-        float unR = ab - 0.5f * slope_un_R * order_mask;
-        float utR = tb - 0.5f * slope_ut_R * order_mask;
-        float pR = b.p - 0.5f * slope_p_R * order_mask;
+        const float aa = XDIR ? a.u : a.v, ab = XDIR ? b.u : b.v;
+        const float ta = XDIR ? a.v : a.u, tb = XDIR ? b.v : b.u;
+        float rhoL = a.rho + 0.5f * sa[0] * order_mask;
+        float unL = aa + 0.5f * sa[1] * order_mask;
+        float utL = ta + 0.5f * sa[2] * order_mask;
+        float pL = a.p + 0.5f * sa[3] * order_mask;
+        float rhoR = b.rho - 0.5f * sb[0] * order_mask;
+        float unR = ab - 0.5f * sb[1] * order_mask;
+        float utR = tb - 0.5f * sb[2] * order_mask;
+        float pR = b.p - 0.5f * sb[3] * order_mask;
         rhoL = fmaxf(rhoL, MIN_DENSITY);
         pL = fmaxf(pL, MIN_PRESSURE);
         rhoR = fmaxf(rhoR, MIN_DENSITY);
@@ -261,6 +264,16 @@ __device__ __forceinline__ void face_flux(bool valid, bool near_wall, const Prim
         out[3] = 0.0f;
         out[4] = 0.0f;
     }
+}
+
+// One face from the four stencil cells m1, a | b, p2.
+template <bool XDIR, int SCHEME, int LIM>
+__device__ __forceinline__ void face_flux(bool valid, bool near_wall, const Prim &m1, const Prim &a, const Prim &b,
+                                          const Prim &p2, float out[5]) {
+    float sa[4], sb[4];
+    cell_slopes<XDIR, LIM>(m1, a, b, sa);
+    cell_slopes<XDIR, LIM>(a, b, p2, sb);
+    face_flux_sl<XDIR, SCHEME>(valid, near_wall, a, sa, b, sb, out);
 }
 
 // updateKernel body for a non-wall cell (src/solver.cu:1736-1875).

@@ -200,6 +200,7 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
     int kr = base % KP, par = (base / KP) & 1, ku = (base + KP - 1) % KP;
     int pc0 = 0, pc1 = 4, pc2 = 2;  // P/M rows of row pairs q, q-1, q-2
     float fyB[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};  // y-face below row r-2
+    float sy2[4] = {0.0f, 0.0f, 0.0f, 0.0f};         // y-slopes of row r-2
     bool ok_all = true;
 
     for (int q = 0; q < npairs; q++) {
@@ -235,12 +236,15 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
         {
             const float4 cp = P[(pc0 + 1) * NT + cy];  // r+1
             const uint32_t my0 = M[pc1 * NT + cy], my1 = M[(pc1 + 1) * NT + cy];
-            face_flux<false, SCHEME, LIM>((my0 & MB_YV) != 0, (my0 & MB_YN) != 0, Prim{c3.x, c3.y, c3.z, c3.w},
-                                          Prim{c2.x, c2.y, c2.z, c2.w}, Prim{c1.x, c1.y, c1.z, c1.w},
-                                          Prim{c0.x, c0.y, c0.z, c0.w}, fy0);
-            face_flux<false, SCHEME, LIM>((my1 & MB_YV) != 0, (my1 & MB_YN) != 0, Prim{c2.x, c2.y, c2.z, c2.w},
-                                          Prim{c1.x, c1.y, c1.z, c1.w}, Prim{c0.x, c0.y, c0.z, c0.w},
-                                          Prim{cp.x, cp.y, cp.z, cp.w}, fy1);
+            // y-slopes of rows r-1 and r; those of row r-2 are row r of step q-1
+            const Prim q2{c2.x, c2.y, c2.z, c2.w}, q1{c1.x, c1.y, c1.z, c1.w}, q0{c0.x, c0.y, c0.z, c0.w};
+            float s1[4], s0[4];
+            cell_slopes<false, LIM>(q2, q1, q0, s1);
+            cell_slopes<false, LIM>(q1, q0, Prim{cp.x, cp.y, cp.z, cp.w}, s0);
+            face_flux_sl<false, SCHEME>((my0 & MB_YV) != 0, (my0 & MB_YN) != 0, q2, sy2, q1, s1, fy0);
+            face_flux_sl<false, SCHEME>((my1 & MB_YV) != 0, (my1 & MB_YN) != 0, q1, s1, q0, s0, fy1);
+#pragma unroll
+            for (int k = 0; k < 4; k++) sy2[k] = s0[k];
         }
 #pragma unroll
         for (int h = 0; h < 2; h++) {

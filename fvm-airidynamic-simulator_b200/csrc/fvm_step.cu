@@ -371,32 +371,40 @@ struct ViscLayout {
     static constexpr int W = NT - 4;
     static constexpr int NB = (NT + 4 + kBox - 1) / kBox;
     static constexpr int BW = NB * kBox;
-    static constexpr int PR = 5;
-    static constexpr int TR = 3;
+    static constexpr int KP = K / 2;   // input ring: K rows staged as K/2 row pairs
+    static constexpr int PP = 3;       // primitive / mask ring (row pairs)
+    static constexpr int TP = 2;       // stress / heat-flux ring (row pairs)
     static constexpr int SLOT = NB * kBoxStride;
     static constexpr size_t raw_off = 0;
     static constexpr size_t raw_bytes = (size_t)K * SLOT * 4;
     static constexpr size_t p_off = raw_off + raw_bytes;
-    static constexpr size_t p_bytes = (size_t)PR * NT * 16;
+    static constexpr size_t p_bytes = (size_t)PP * 2 * NT * 16;
     static constexpr size_t t_off = p_off + p_bytes;
-    static constexpr size_t t_bytes = (size_t)TR * 5 * NT * 4;
+    static constexpr size_t t_bytes = (size_t)TP * 2 * 5 * NT * 4;
     static constexpr size_t m_off = t_off + t_bytes;
-    static constexpr size_t m_bytes = (size_t)PR * NT;
+    static constexpr size_t m_bytes = (size_t)PP * 2 * NT;
     static constexpr size_t bar_off = (m_off + m_bytes + 15) & ~(size_t)15;
-    static constexpr size_t total = bar_off + K * 8 + 128;  // + alignment slack
-    static constexpr uint32_t tx_bytes = 5 * BW * 4;
+    static constexpr size_t total = bar_off + KP * 8 + 128;  // + alignment slack
+    static constexpr uint32_t tx_bytes = 2 * 5 * BW * 4;  // one row pair
 };
 
 // Viscous half step on one tile (fusedViscousDiffusionKernel,
-// src/solver.cu:2251-2511), out of place: primitives (u, v, T) of the input
-// on NT columns, stress/heat flux on NT-2 columns, update on W = NT-4.
+// src/solver.cu:2251-2511), out of place, marching two rows per step.
+// Per step q (incoming rows r = j0-2+2q and r+1):
+//   phase 1  primitives (u, v, T) + masks of rows r, r+1 on NT columns; the
+//            thread also keeps the conserved state of rows r, r+1 at the
+//            column it updates one step later, so the input slot is free
+//            after the first barrier and is refilled there
+//   -- barrier --
+//   phase 2  stress and heat flux of rows r-1, r on NT-2 columns
+//   -- barrier --
+//   phase 3  viscous update of rows r-2, r-1 on W columns
 template <int NT, int K>
 __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const StepArgs &a, int i0, int j0,
                                              unsigned char *smem, RingPos &rp, float &lmax_speed, float &lmax_nu) {
     using L = ViscLayout<NT, K>;
-    constexpr int W = L::W, PR = L::PR, TR = L::TR;
-    static_assert(PR == 5 && TR == 3, "ring sizes");
-    constexpr int AHEAD = K - 3;
+    constexpr int W = L::W, KP = L::KP;
+    static_assert(L::PP == 3 && L::TP == 2 && KP >= 2, "ring sizes");
     float *raw = reinterpret_cast<float *>(smem + L::raw_off);
     float4 *P = reinterpret_cast<float4 *>(smem + L::p_off);  // {u, v, T, -}
     float *Tq = reinterpret_cast<float *>(smem + L::t_off);   // {txx, tyy, txy, qx, qy}
@@ -408,7 +416,7 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
     const int t = threadIdx.x;
     const int j1 = min(j0 + a.rows_per_cta, ny);
     const int rs = j0 - 2;
-    const int nrows = (j1 + 1) - rs + 1;
+    const int npairs = (j1 - j0 + 5) / 2;  // incoming rows rs .. j1+1 (one spare row when odd)
     const float dt = a.sc->dt * a.dt_scale;
     ViscArgs va;
     va.inv_2dx = 0.5f / g.dx;
@@ -420,150 +428,189 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
 
     fence_proxy_async_smem();
     __syncthreads();
-    const int base = rp.base;
-    int islot = base % K;
+    const int base = rp.base;  // row pairs this CTA staged before this tile
+    int islot = base % KP;
     auto issue = [&](int q) {
-        const int row = clampi(rs + q, 0, ny - 1);
         mbar_arrive_expect_tx(&bars[islot], L::tx_bytes);
 #pragma unroll
-        for (int b = 0; b < L::NB; b++)
-            tma_load_3d(raw + (size_t)islot * L::SLOT + b * kBoxStride, tm_in, &bars[islot], i0 - 4 + b * kBox, row,
-                        0);
-        islot = ring_next<K>(islot);
+        for (int h = 0; h < 2; h++) {
+            const int row = clampi(rs + 2 * q + h, 0, ny - 1);
+            float *dst = raw + (size_t)(islot * 2 + h) * L::SLOT;
+#pragma unroll
+            for (int b = 0; b < L::NB; b++)
+                tma_load_3d(dst + b * kBoxStride, tm_in, &bars[islot], i0 - 4 + b * kBox, row, 0);
+        }
+        islot = ring_next<KP>(islot);
     };
-    int issued = min(AHEAD, nrows);
+    int issued = min(KP, npairs);
     if (t == 0)
         for (int q = 0; q < issued; q++) issue(q);
 
     const int ic_t = clampi(i0 - 2 + t, 0, nx - 1);
     const int rc_t = ic_t - i0 + 4;
     const uint8_t *mcol = a.mask + ic_t;
-    uint32_t m_cur = __ldg(mcol + (size_t)clampi(rs, 0, ny - 1) * g.pitch);
-    uint32_t m_nxt = __ldg(mcol + (size_t)clampi(rs + 1, 0, ny - 1) * g.pitch);
+    uint32_t mA = __ldg(mcol + (size_t)clampi(rs, 0, ny - 1) * g.pitch);
+    uint32_t mB = __ldg(mcol + (size_t)clampi(rs + 1, 0, ny - 1) * g.pitch);
     const int is = i0 - 1 + t;
     const bool stress_col_in = (t < NT - 2) && is >= 0 && is < nx;
     const int iu = i0 + t;
     const bool col_ok = (t < W) && (iu < nx);
     const bool interior_x = iu > 0 && iu < nx - 1;
+    const int uc = min(t, W - 1) + 4;  // staged column of the updated cell
     float *outp = a.out + iu;
 
-    int kr = base % K, par = (base / K) & 1, ku = (base + K - 2) % K;
-    int p0 = 0, p1 = PR - 1, p2 = PR - 2, p3 = PR - 3;
-    int s1 = 0, s2 = TR - 1, s3 = TR - 2;
+    int kr = base % KP, par = (base / KP) & 1;
+    int pc0 = 0, pc1 = 4, pc2 = 2;  // P/M rows of row pairs q, q-1, q-2
+    int tc0 = 0, tc1 = 2;           // stress rows of row pairs q (rows r-1, r) and q-1
+    float Uprev[2][5];              // conserved state of rows r-2, r-1 at column iu
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+#pragma unroll
+        for (int k = 0; k < 5; k++) Uprev[h][k] = 0.0f;
     bool ok_all = true;
 
-    for (int q = 0; q < nrows; q++) {
-        const int r = rs + q;
-        const uint32_t m_pf = __ldg(mcol + (size_t)clampi(r + 2, 0, ny - 1) * g.pitch);
+    for (int q = 0; q < npairs; q++) {
+        const int r = rs + 2 * q;
+        const uint32_t nA = __ldg(mcol + (size_t)clampi(r + 2, 0, ny - 1) * g.pitch);
+        const uint32_t nB = __ldg(mcol + (size_t)clampi(r + 3, 0, ny - 1) * g.pitch);
+        // ---- phase 1: primitives + masks of rows r, r+1; conserved state for step q+1
+        float Unext[2][5];
         bool ok = mbar_wait_bounded(&bars[kr], (uint32_t)par);
         if (ok) {
-            const float *src = raw + (size_t)kr * L::SLOT;
-            float u, v, p, T;
-            prim_from_cons(ring_at<L::NB>(src, 0, rc_t), ring_at<L::NB>(src, 1, rc_t), ring_at<L::NB>(src, 2, rc_t),
-                           ring_at<L::NB>(src, 3, rc_t), ring_at<L::NB>(src, 4, rc_t), u, v, p, T);
-            P[p0 * NT + t] = make_float4(u, v, T, 0.0f);
-            M[p0 * NT + t] = (uint8_t)m_cur;
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const float *src = raw + (size_t)(kr * 2 + h) * L::SLOT;
+                float u, v, p, T;
+                prim_from_cons(ring_at<L::NB>(src, 0, rc_t), ring_at<L::NB>(src, 1, rc_t),
+                               ring_at<L::NB>(src, 2, rc_t), ring_at<L::NB>(src, 3, rc_t),
+                               ring_at<L::NB>(src, 4, rc_t), u, v, p, T);
+                P[(pc0 + h) * NT + t] = make_float4(u, v, T, 0.0f);
+                M[(pc0 + h) * NT + t] = (uint8_t)(h ? mB : mA);
+#pragma unroll
+                for (int k = 0; k < 5; k++) Unext[h][k] = ring_at<L::NB>(src, k, uc);
+            }
+        } else {
+#pragma unroll
+            for (int h = 0; h < 2; h++)
+#pragma unroll
+                for (int k = 0; k < 5; k++) Unext[h][k] = 0.0f;
         }
-        m_cur = m_nxt;
-        m_nxt = m_pf;
+        mA = nA;
+        mB = nB;
+        fence_proxy_async_smem();
         if (__syncthreads_or(!ok)) {
             ok_all = false;
             break;
         }
-        // ---- phase 2: stress and heat flux of row r-1 at column i0-1+t
-        const int trow = r - 1;
-        if (trow >= j0 - 1 && t < NT - 2) {
-            const int c = t + 1;
-            float out[5];
-            const uint32_t ct = mb_type(M[p1 * NT + c]);
-            if (!stress_col_in || trow < 0 || trow >= ny || ct == CT_SOLID) {
-#pragma unroll
-                for (int k = 0; k < 5; k++) out[k] = 0.0f;
-            } else {
-                const float4 C = P[p1 * NT + c], E = P[p1 * NT + c + 1], Wc = P[p1 * NT + c - 1];
-                const float4 N = P[p0 * NT + c], S = P[p2 * NT + c];
-                stress_heat(C.x, C.y, C.z, E.x, Wc.x, N.x, S.x, E.y, Wc.y, N.y, S.y, E.z, Wc.z, N.z, S.z, is == 0,
-                            is == nx - 1, trow == 0, trow == ny - 1, va, out);
-            }
-            float *Ts = Tq + s1 * 5 * NT + t;
-#pragma unroll
-            for (int k = 0; k < 5; k++) Ts[k * NT] = out[k];
-        }
-        fence_proxy_async_smem();
-        __syncthreads();
-        if (t == 0 && issued < nrows && issued <= q + AHEAD) {
+        // the input slot of pair q is free now: stage pair q+KP into it
+        if (t == 0 && issued < npairs && issued <= q + KP) {
             issue(issued);
             ++issued;
         }
-        // ---- phase 3: viscous update of row r-2 at column i0+t
-        const int urow = r - 2;
-        if (urow >= j0 && urow < j1 && col_ok) {
-            const int c = t + 2;   // primitive column
-            const int tc = t + 1;  // stress column
-            const uint32_t mb = M[p2 * NT + c];
-            const uint32_t ctype = mb_type(mb);
-            const float *src = raw + (size_t)ku * L::SLOT;
-            float U[5];
+        // ---- phase 2: stress and heat flux of rows r-1, r at column i0-1+t
+        if (t < NT - 2) {
+            const int c = t + 1;
 #pragma unroll
-            for (int k = 0; k < 5; k++) U[k] = ring_at<L::NB>(src, k, t + 4);
-            const float4 pc = P[p2 * NT + c];
-            if (ctype == CT_FLUID && interior_x && urow > 0 && urow < ny - 1) {
-                const float *T0 = Tq + s2 * 5 * NT + tc;
-                const float *TN = Tq + s1 * 5 * NT + tc;
-                const float *TS = Tq + s3 * 5 * NT + tc;
-                float tC[5], tE[5], tW[5], tNn[5], tSs[5];
+            for (int h = 0; h < 2; h++) {
+                const int trow = r - 1 + h;
+                if (trow >= j0 - 1) {
+                    // rows trow-1, trow, trow+1 of the primitive ring
+                    const int rowS = h ? pc1 + 1 : pc1, rowC = h ? pc0 : pc1 + 1, rowN = h ? pc0 + 1 : pc0;
+                    float out[5];
+                    const uint32_t ct = mb_type(M[rowC * NT + c]);
+                    if (!stress_col_in || trow < 0 || trow >= ny || ct == CT_SOLID) {
 #pragma unroll
-                for (int k = 0; k < 5; k++) {
-                    tC[k] = T0[k * NT];
-                    tE[k] = T0[k * NT + 1];
-                    tW[k] = T0[k * NT - 1];
-                    tNn[k] = TN[k * NT];
-                    tSs[k] = TS[k * NT];
-                }
-                const float4 E = P[p2 * NT + c + 1], Wc = P[p2 * NT + c - 1];
-                const float4 N = P[p1 * NT + c];
-                const float4 S = P[p3 * NT + c];
-                float rhs[4];
-                viscous_rhs(tC, tE, tW, tNn, tSs, E.x, Wc.x, N.x, S.x, E.y, Wc.y, N.y, S.y, va, rhs);
-                U[1] += dt * rhs[0];
-                U[2] += dt * rhs[1];
-                U[3] += dt * rhs[2];
-                U[4] += dt * rhs[3];
-            }
-            if (a.apply_bc) bc_pointwise(U, ctype, iu, urow, nx, ny, a.fs);
-            if (a.cfl && ctype != CT_GHOST) {
-                float uu, vv, pp, TT;
-                prim_from_cons(U[0], U[1], U[2], U[3], U[4], uu, vv, pp, TT);
-                lmax_speed = fmaxf(lmax_speed, wave_speed(uu, vv, pp, U[0]));
-                if (a.cfl == 2) {
-                    const float mu = (ctype == CT_SOLID) ? 0.0f : sutherland_mu(pc.z);
-                    lmax_nu = fmaxf(lmax_nu, mu / (U[0] + 1e-10f));
+                        for (int k = 0; k < 5; k++) out[k] = 0.0f;
+                    } else {
+                        const float4 C = P[rowC * NT + c], E = P[rowC * NT + c + 1], Wc = P[rowC * NT + c - 1];
+                        const float4 N = P[rowN * NT + c], S = P[rowS * NT + c];
+                        stress_heat(C.x, C.y, C.z, E.x, Wc.x, N.x, S.x, E.y, Wc.y, N.y, S.y, E.z, Wc.z, N.z, S.z,
+                                    is == 0, is == nx - 1, trow == 0, trow == ny - 1, va, out);
+                    }
+                    float *Ts = Tq + (tc0 + h) * 5 * NT + t;
+#pragma unroll
+                    for (int k = 0; k < 5; k++) Ts[k * NT] = out[k];
                 }
             }
-            float *dst = outp + (size_t)urow * g.pitch;
-#pragma unroll
-            for (int k = 0; k < 5; k++) dst[k * g.plane] = U[k];
         }
-        kr = ring_next<K>(kr);
+        // south neighbour of row r-2 (row r-3, pair q-2): read before its slot is reused
+        const float4 S0 = P[(pc2 + 1) * NT + min(t, W - 1) + 2];
+        __syncthreads();
+        // ---- phase 3: viscous update of rows r-2, r-1 at column i0+t
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int urow = r - 2 + h;
+            if (urow >= j0 && urow < j1 && col_ok) {
+                const int c = t + 2;   // primitive column
+                const int tc = t + 1;  // stress column
+                const int prow = pc1 + h;
+                const uint32_t mb = M[prow * NT + c];
+                const uint32_t ctype = mb_type(mb);
+                float U[5];
+#pragma unroll
+                for (int k = 0; k < 5; k++) U[k] = Uprev[h][k];
+                const float4 pc = P[prow * NT + c];
+                if (ctype == CT_FLUID && interior_x && urow > 0 && urow < ny - 1) {
+                    // stress rows urow-1, urow, urow+1
+                    const int tS = h ? tc1 + 1 : tc1, tC0 = h ? tc0 : tc1 + 1, tN = h ? tc0 + 1 : tc0;
+                    const float *T0 = Tq + tC0 * 5 * NT + tc;
+                    const float *TN = Tq + tN * 5 * NT + tc;
+                    const float *TS = Tq + tS * 5 * NT + tc;
+                    float tC[5], tE[5], tW[5], tNn[5], tSs[5];
+#pragma unroll
+                    for (int k = 0; k < 5; k++) {
+                        tC[k] = T0[k * NT];
+                        tE[k] = T0[k * NT + 1];
+                        tW[k] = T0[k * NT - 1];
+                        tNn[k] = TN[k * NT];
+                        tSs[k] = TS[k * NT];
+                    }
+                    const float4 E = P[prow * NT + c + 1], Wc = P[prow * NT + c - 1];
+                    const float4 N = P[(h ? pc0 : pc1 + 1) * NT + c];
+                    const float4 S = h ? P[pc1 * NT + c] : S0;
+                    float rhs[4];
+                    viscous_rhs(tC, tE, tW, tNn, tSs, E.x, Wc.x, N.x, S.x, E.y, Wc.y, N.y, S.y, va, rhs);
+                    U[1] += dt * rhs[0];
+                    U[2] += dt * rhs[1];
+                    U[3] += dt * rhs[2];
+                    U[4] += dt * rhs[3];
+                }
+                if (a.apply_bc) bc_pointwise(U, ctype, iu, urow, nx, ny, a.fs);
+                if (a.cfl && ctype != CT_GHOST) {
+                    float uu, vv, pp, TT;
+                    prim_from_cons(U[0], U[1], U[2], U[3], U[4], uu, vv, pp, TT);
+                    lmax_speed = fmaxf(lmax_speed, wave_speed(uu, vv, pp, U[0]));
+                    if (a.cfl == 2) {
+                        const float mu = (ctype == CT_SOLID) ? 0.0f : sutherland_mu(pc.z);
+                        lmax_nu = fmaxf(lmax_nu, mu / (U[0] + 1e-10f));
+                    }
+                }
+                float *dst = outp + (size_t)urow * g.pitch;
+#pragma unroll
+                for (int k = 0; k < 5; k++) dst[k * g.plane] = U[k];
+            }
+        }
+#pragma unroll
+        for (int h = 0; h < 2; h++)
+#pragma unroll
+            for (int k = 0; k < 5; k++) Uprev[h][k] = Unext[h][k];
+        kr = ring_next<KP>(kr);
         par ^= (kr == 0) ? 1 : 0;
-        ku = ring_next<K>(ku);
-        p3 = p2;
-        p2 = p1;
-        p1 = p0;
-        p0 = ring_next<PR>(p0);
-        s3 = s2;
-        s2 = s1;
-        s1 = ring_next<TR>(s1);
+        pc2 = pc1;
+        pc1 = pc0;
+        pc0 = (pc0 == 4) ? 0 : pc0 + 2;
+        tc1 = tc0;
+        tc0 = 2 - tc0;
     }
     if (!ok_all) {
         if (t == 0) {
             record_error(a.sc, kErrTimeout);
             for (int q = 0; q < issued; q++)
-                mbar_wait_bounded(&bars[(base + q) % K], (uint32_t)(((base + q) / K) & 1), 20000000LL);
+                mbar_wait_bounded(&bars[(base + q) % KP], (uint32_t)(((base + q) / KP) & 1), 20000000LL);
         }
         return false;
     }
-    rp.base = base + nrows;
+    rp.base = base + npairs;
     return true;
 }
 
@@ -576,7 +623,7 @@ __global__ void __launch_bounds__(NT) k_viscous(const __grid_constant__ CUtensor
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bar_off);
     if (threadIdx.x == 0) {
         prefetch_tensormap(&tm_in);
-        for (int k = 0; k < K; k++) mbar_init(&bars[k], 1);
+        for (int k = 0; k < L::KP; k++) mbar_init(&bars[k], 1);
         fence_barrier_init();
     }
     RingPos rp{0};
@@ -666,7 +713,7 @@ __global__ void __launch_bounds__(NT) k_viscous_batch(const BatchInst *__restric
     if (smem_misaligned(smem, insts[0].sc)) return;
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bar_off);
     if (threadIdx.x == 0) {
-        for (int k = 0; k < K; k++) mbar_init(&bars[k], 1);
+        for (int k = 0; k < L::KP; k++) mbar_init(&bars[k], 1);
         fence_barrier_init();
     }
     RingPos rp{0};

@@ -13,7 +13,7 @@ import os
 
 import numpy as np
 
-from .abi import (SimParams, Ext, Diag, KernelTime, Result, ServerStats, STATUS, params_default, compute_derived,
+from .abi import (SimParams, Ext, Diag, KernelTime, Result, ServerStats, Shedding, STATUS, params_default, compute_derived,
                   ext_default, workload)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -33,7 +33,7 @@ EXPORTS = [
     "fvm_batch_read_fields", "fvm_batch_diagnostics", "fvm_batch_memory_usage", "fvm_batch_launch_count",
     "fvm_batch_instance_bytes", "fvm_batch_retire", "fvm_batch_trim", "fvm_server_create", "fvm_server_submit",
     "fvm_server_poll", "fvm_server_wait", "fvm_server_drain", "fvm_server_get_stats", "fvm_server_destroy",
-    "fvm_state_max_noalloc", "fvm_autotune", "fvm_get_tune", "fvm_debug_stage1", "fvm_debug_ghost_table", "fvm_build_info",
+    "fvm_state_max_noalloc", "fvm_shedding_stats", "fvm_autotune", "fvm_get_tune", "fvm_debug_stage1", "fvm_debug_ghost_table", "fvm_build_info",
 ]
 
 
@@ -115,6 +115,8 @@ def load_library(path=None):
     lib.fvm_batch_instance_bytes.argtypes = [i, i]
     lib.fvm_batch_instance_bytes.restype = sz
     lib.fvm_state_max_noalloc.argtypes = [vp, i, i, sz, sz, i, fp, vp]
+    dp = C.POINTER(C.c_double)
+    lib.fvm_shedding_stats.argtypes = [dp, dp, dp, i, C.c_double, C.c_double, C.POINTER(Shedding)]
     lib.fvm_batch_retire.argtypes = [vp, i]
     lib.fvm_batch_trim.argtypes = [vp, sz, C.POINTER(sz)]
     lib.fvm_server_create.argtypes = [C.POINTER(vp), C.POINTER(Ext), sz, i, i]
@@ -466,6 +468,19 @@ class Server:
         return st
 
 
+def shedding_stats(t, cd, cl, ref_length, u_inf):
+    """Strouhal number and cycle-averaged drag/lift of a force history
+    (fvm_shedding_stats); t, cd, cl: equal-length sequences."""
+    t, cd, cl = (np.ascontiguousarray(x, dtype=np.float64) for x in (t, cd, cl))
+    if not (len(t) == len(cd) == len(cl)):
+        raise FvmError(1, "t, cd, cl must have equal lengths")
+    out = Shedding()
+    dp = C.POINTER(C.c_double)
+    _check(load_library().fvm_shedding_stats(t.ctypes.data_as(dp), cd.ctypes.data_as(dp), cl.ctypes.data_as(dp),
+                                             len(t), float(ref_length), float(u_inf), C.byref(out)))
+    return out
+
+
 def instance_bytes(nx, ny):
     return load_library().fvm_batch_instance_bytes(int(nx), int(ny))
 
@@ -477,5 +492,5 @@ def gpu_mem_info():
     return f.value, t.value
 
 
-__all__ = ["Solver", "Batch", "Server", "instance_bytes", "FvmError", "SimParams", "Ext", "Diag", "params_default", "compute_derived",
+__all__ = ["Solver", "Batch", "Server", "shedding_stats", "instance_bytes", "FvmError", "SimParams", "Ext", "Diag", "params_default", "compute_derived",
            "ext_default", "workload", "load_library", "gpu_mem_info", "EXPORTS", "LIB_PATH"]

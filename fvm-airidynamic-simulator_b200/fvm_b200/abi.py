@@ -79,6 +79,12 @@ class ServerStats(C.Structure):
                 ("step_ms_p99", C.c_double), ("step_ms_mean", C.c_double), ("reserved", C.c_double * 4)]
 
 
+class Shedding(C.Structure):
+    """fvm_shedding: vortex-shedding statistics of a force history."""
+    _fields_ = [("strouhal", C.c_double), ("period", C.c_double), ("cd_mean", C.c_double), ("cl_mean", C.c_double),
+                ("cl_rms", C.c_double), ("cycles", C.c_int), ("reserved", C.c_int)]
+
+
 class KernelTime(C.Structure):
     _fields_ = [("name", C.c_char * 48), ("launches", C.c_longlong), ("total_ms", C.c_double)]
 

@@ -335,6 +335,21 @@ int fvm_server_destroy(fvm_server *s);
 int fvm_state_max_noalloc(const float *state, int nx, int ny, size_t pitch, size_t plane, int what, float *out,
                           void *stream);
 
+/* ------------------------------------------------------------ analysis
+ * Vortex-shedding statistics of a force-coefficient history (samples at
+ * strictly increasing times t; cd, cl from fvm_diagnostics), for the
+ * Strouhal number of a cylinder wake.  Whole cycles between the first and
+ * last upward zero crossing of cl - mean(cl) give the period, St =
+ * ref_length / (period * u_inf), and the cycle-averaged drag and lift.
+ * Host code, no device work.  No reference counterpart. */
+typedef struct {
+    double strouhal, period, cd_mean, cl_mean, cl_rms;
+    int cycles;    /* whole shedding cycles used */
+    int reserved;
+} fvm_shedding;
+int fvm_shedding_stats(const double *t, const double *cd, const double *cl, int n, double ref_length, double u_inf,
+                       fvm_shedding *out);
+
 /* Count of kernels this library launched on the handle since creation. */
 int fvm_launch_count(fvm_handle *h, long long *count_out);
 

@@ -1,0 +1,111 @@
+"""Long-run and full-size checks against the oracle.
+
+* Config 1 at its stated size: 512x256 Euler, Mach 3, circle, 200 steps,
+  HLLC (the reference's flux) and AUSM+, against the FP32 oracle (L1 1e-4
+  through shocks) with the FP64 oracle's distance stated.
+* Vortex street (Re 200, Mach 0.3) on a reduced 256x128 grid: Strouhal
+  number and cycle-mean drag over whole shedding cycles within 0.5 % of the
+  FP64 oracle.
+* Hypersonic blunted cone (Mach 8, Re 1e5, isothermal wall) on a reduced
+  512x256 grid: bow-shock standoff, integrated wall heat flux and drag within
+  0.5 % of the FP64 oracle after 2000 steps.
+Both solves use the recompute-dt policy (each step's dt from the CFL of its
+start state) and start from the same geometry and state."""
+import os
+
+import numpy as np
+import pytest
+
+from helpers import rel_l1, small, FIELDS
+
+pytestmark = pytest.mark.gpu
+
+import fvm_b200  # noqa: E402
+from fvm_b200 import abi  # noqa: E402
+from oracle.oracle import Oracle  # noqa: E402
+
+THREADS = os.cpu_count() or 1
+
+
+def _twins(p, e, bits):
+    s = fvm_b200.Solver(abi.SimParams.from_buffer_copy(p), abi.Ext.from_buffer_copy(e))
+    o = Oracle(p, e, bits=bits, threads=THREADS)
+    o.set_geometry(s.sdf(), s.cell_types())
+    o.set_fields(s.fields())
+    return s, o
+
+
+@pytest.mark.parametrize("flux", [abi.FLUX_HLLC, abi.FLUX_AUSM_PLUS])
+def test_config1_full_size_200_steps(flux):
+    p, e = small("euler_m3_circle", 512, 256, flux_scheme=flux)
+    e.dt_policy = abi.DT_RECOMPUTE
+    s, o32 = _twins(p, e, 32)
+    s.step(200)
+    o32.run(200, recompute=True)
+    U = s.fields()
+    err32 = rel_l1(U, o32.fields())
+    assert np.isfinite(U).all()
+    assert err32.max() <= 1e-4, dict(zip(FIELDS, err32))
+    _, o64 = _twins(p, e, 64)
+    o64.run(200, recompute=True)
+    err64 = rel_l1(U, o64.fields())  # stated FP32-vs-FP64 distance of the method
+    assert err64.max() <= 1e-3, dict(zip(FIELDS, err64))
+
+
+def _history_gpu(s, warm, samples, every):
+    s.step(warm)
+    t, cd, cl = [], [], []
+    for _ in range(samples):
+        s.step(every)
+        d = s.diagnostics()
+        t.append(s.params.t_current)
+        cd.append(d.cd)
+        cl.append(d.cl)
+    return np.array(t), np.array(cd), np.array(cl)
+
+
+def _history_oracle(o, warm, samples, every):
+    tt = 0.0
+    for _ in range(warm):
+        dt = o.compute_dt()
+        o.step(dt)
+        tt += dt
+    t, cd, cl = [], [], []
+    for _ in range(samples):
+        for _ in range(every):
+            dt = o.compute_dt()
+            o.step(dt)
+            tt += dt
+        d = o.diagnostics()
+        t.append(tt)
+        cd.append(d.cd)
+        cl.append(d.cl)
+    return np.array(t), np.array(cd), np.array(cl)
+
+
+def test_vortex_street_strouhal_and_drag_match_fp64_oracle():
+    p, e = abi.workload("ns_karman_re200", 256, 128)
+    e.dt_policy = abi.DT_RECOMPUTE
+    s, o = _twins(p, e, 64)
+    warm, samples, every = 4000, 800, 10  # ~11 shedding cycles after the start-up
+    g = fvm_b200.shedding_stats(*_history_gpu(s, warm, samples, every), e.ref_length, p.u_inf)
+    r = fvm_b200.shedding_stats(*_history_oracle(o, warm, samples, every), e.ref_length, p.u_inf)
+    assert g.cycles >= 8 and r.cycles >= 8
+    assert abs(g.strouhal - r.strouhal) <= 5e-3 * r.strouhal, (g.strouhal, r.strouhal)
+    assert abs(g.cd_mean - r.cd_mean) <= 5e-3 * abs(r.cd_mean), (g.cd_mean, r.cd_mean)
+    assert 0.1 < g.strouhal < 0.3 and g.cl_rms > 0.1
+
+
+def test_cone_standoff_heat_and_drag_match_fp64_oracle():
+    p, e = abi.workload("ns_hypersonic_cone", 512, 256)
+    e.dt_policy = abi.DT_RECOMPUTE
+    s, o = _twins(p, e, 64)
+    s.step(2000)
+    o.run(2000, recompute=True)
+    dg, do = s.diagnostics(), o.diagnostics()
+    sg, so = s.shock_standoff(), o.shock_standoff()
+    assert so > 0 and abs(sg - so) <= 5e-3 * so, (sg, so)
+    assert abs(dg.wall_heat - do.wall_heat) <= 5e-3 * abs(do.wall_heat), (dg.wall_heat, do.wall_heat)
+    assert abs(dg.cd - do.cd) <= 5e-3 * abs(do.cd), (dg.cd, do.cd)
+    # FP32 state, FP64 totals: mass drifts from the FP64 solve by < 1e-3 over 2000 steps
+    assert abs(dg.mass - do.mass) <= 1e-3 * do.mass

@@ -20,27 +20,19 @@ __global__ void k_primitives(GridDesc g, const float *U, float *u, float *v, flo
 }
 
 // compute{Temperature,Pressure,VelocityMag,Mach}DirectKernel and the density
-// copy (src/solver.cu:3527-3671); dense nx*ny destination.
-__global__ void k_derived(int kind, GridDesc g, const float *U, float *dst) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    int j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= g.nx || j >= g.ny) return;
-    size_t c = (size_t)j * g.pitch + i, d = (size_t)j * g.nx + i;
-    const float rho = U[c], rho_u = U[g.plane + c], rho_v = U[2 * g.plane + c], rho_e = U[4 * g.plane + c];
-    float out;
+// copy (src/solver.cu:3527-3671): the derived value of one cell.
+__device__ __forceinline__ float derived_value(int kind, float rho, float rho_u, float rho_v, float rho_e) {
     switch (kind) {
     case 0: {
         float e = rho_e / (rho + 1e-10f);
-        out = (GAMMA - 1.0f) * e / R_GAS;
-        break;
+        return (GAMMA - 1.0f) * e / R_GAS;
     }
-    case 1: out = (GAMMA - 1.0f) * rho_e; break;
-    case 2: out = rho; break;
+    case 1: return (GAMMA - 1.0f) * rho_e;
+    case 2: return rho;
     case 3: {
         float rv = rho + 1e-10f;
         float u = rho_u / rv, v = rho_v / rv;
-        out = sqrtf(u * u + v * v);
-        break;
+        return sqrtf(u * u + v * v);
     }
     default: {
         float rv = rho + 1e-10f;
@@ -49,11 +41,52 @@ __global__ void k_derived(int kind, GridDesc g, const float *U, float *dst) {
         float e = rho_e / rv;
         float T = (GAMMA - 1.0f) * e / R_GAS;
         float cs = sqrtf(GAMMA * R_GAS * T);
-        out = speed / (cs + 1e-10f);
-        break;
+        return speed / (cs + 1e-10f);
     }
     }
-    dst[d] = out;
+}
+
+// Derived field into a dense nx*ny destination.
+__global__ void k_derived(int kind, GridDesc g, const float *U, float *dst) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= g.nx || j >= g.ny) return;
+    size_t c = (size_t)j * g.pitch + i, d = (size_t)j * g.nx + i;
+    dst[d] = derived_value(kind, U[c], U[g.plane + c], U[2 * g.plane + c], U[4 * g.plane + c]);
+}
+
+// The renderer's field pass (FIELD_FRAGMENT_SHADER, src/renderer.cpp:47-77)
+// with one pixel per cell: SOLID and GHOST cells dark grey, others the
+// derived value normalised by (v - lo) / (hi - lo + 1e-4), clamped to [0, 1],
+// then looked up in the 256-entry colour table the way a linearly filtered,
+// edge-clamped 1-D texture samples it.  fmt 0: RGBA float, fmt 1: RGBA8.
+__global__ void k_colormap(int kind, GridDesc g, const float *U, const uint8_t *ct,
+                           const __grid_constant__ ColormapLUT lut, float lo, float hi, void *out, int fmt) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= g.nx || j >= g.ny) return;
+    const size_t c = (size_t)j * g.pitch + i, d = (size_t)j * g.nx + i;
+    const uint8_t t = ct[d];
+    float r, gr, b;
+    if (t == CT_SOLID || t == CT_GHOST) {
+        r = gr = b = 0.3f;
+    } else {
+        const float v = derived_value(kind, U[c], U[g.plane + c], U[2 * g.plane + c], U[4 * g.plane + c]);
+        const float s = fminf(fmaxf((v - lo) / (hi - lo + 0.0001f), 0.0f), 1.0f);
+        const float u = s * 256.0f - 0.5f;
+        const float fl = floorf(u);
+        const float a = u - fl;
+        const int i0 = min(max((int)fl, 0), 255), i1 = min(max((int)fl + 1, 0), 255);
+        r = (1.0f - a) * lut.rgb[3 * i0] + a * lut.rgb[3 * i1];
+        gr = (1.0f - a) * lut.rgb[3 * i0 + 1] + a * lut.rgb[3 * i1 + 1];
+        b = (1.0f - a) * lut.rgb[3 * i0 + 2] + a * lut.rgb[3 * i1 + 2];
+    }
+    if (fmt == 0) {
+        reinterpret_cast<float4 *>(out)[d] = make_float4(r, gr, b, 1.0f);
+    } else {
+        auto q = [](float x) { return (unsigned)__float2int_rn(fminf(fmaxf(x, 0.0f), 1.0f) * 255.0f); };
+        reinterpret_cast<uchar4 *>(out)[d] = make_uchar4(q(r), q(gr), q(b), 255);
+    }
 }
 
 // cellTypeToFloatKernel (src/solver.cu:3444-3450)
@@ -278,6 +311,13 @@ cudaError_t launch_primitives(const GridDesc &g, const float *U, float *u, float
                               cudaStream_t st) {
     dim3 b(32, 8);
     k_primitives<<<grid2d(g, b), b, 0, st>>>(g, U, u, v, p, T);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_colormap(int kind, const GridDesc &g, const float *U, const uint8_t *ct, const ColormapLUT &lut,
+                            float lo, float hi, void *out, int fmt, cudaStream_t st) {
+    dim3 b(32, 8);
+    k_colormap<<<grid2d(g, b), b, 0, st>>>(kind, g, U, ct, lut, lo, hi, out, fmt);
     return cudaGetLastError();
 }
 

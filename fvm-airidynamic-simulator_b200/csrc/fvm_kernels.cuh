@@ -61,6 +61,12 @@ int stage_box_blend(const StageTune &tn);      // TMA box width of the blend par
 cudaError_t launch_primitives(const GridDesc &g, const float *U, float *u, float *v, float *p, float *T,
                               cudaStream_t st);  // dense nx*ny outputs
 cudaError_t launch_derived(int kind, const GridDesc &g, const float *U, float *dst, cudaStream_t st);
+// 256-entry RGB colour table, passed to the kernel by value.
+struct ColormapLUT {
+    float rgb[256 * 3];
+};
+cudaError_t launch_colormap(int kind, const GridDesc &g, const float *U, const uint8_t *ct, const ColormapLUT &lut,
+                            float lo, float hi, void *out, int fmt, cudaStream_t st);
 cudaError_t launch_ct_to_float(const GridDesc &g, const uint8_t *ct, float *dst, cudaStream_t st);
 cudaError_t launch_max_reduce(int what, const GridDesc &g, const float *U, float *out_dev, cudaStream_t st);
 cudaError_t launch_arrows_cap(const GridDesc &g, const float *U, float *vertex, int cap, int *counter, int step,

@@ -33,7 +33,7 @@ EXPORTS = [
     "fvm_batch_read_fields", "fvm_batch_diagnostics", "fvm_batch_memory_usage", "fvm_batch_launch_count",
     "fvm_batch_instance_bytes", "fvm_batch_retire", "fvm_batch_trim", "fvm_server_create", "fvm_server_submit",
     "fvm_server_poll", "fvm_server_wait", "fvm_server_drain", "fvm_server_get_stats", "fvm_server_destroy",
-    "fvm_state_max_noalloc", "fvm_shedding_stats", "fvm_autotune", "fvm_get_tune", "fvm_debug_stage1", "fvm_debug_ghost_table", "fvm_build_info",
+    "fvm_state_max_noalloc", "fvm_shedding_stats", "fvm_colormap_to_device", "fvm_colormap_table", "fvm_autotune", "fvm_get_tune", "fvm_debug_stage1", "fvm_debug_ghost_table", "fvm_build_info",
 ]
 
 
@@ -86,6 +86,8 @@ def load_library(path=None):
     lib.fvm_write_fields.argtypes = [vp] + [vp] * 5
     lib.fvm_read_primitives.argtypes = [vp] + [vp] * 4
     lib.fvm_field_to_device.argtypes = [vp, i, vp]
+    lib.fvm_colormap_to_device.argtypes = [vp, i, i, f, f, vp, i]
+    lib.fvm_colormap_table.argtypes = [i, vp]
     lib.fvm_cell_types_to_device.argtypes = [vp, vp]
     lib.fvm_vector_arrows.argtypes = [vp, vp, i, i, f, f, f, f, C.POINTER(i)]
     lib.fvm_max_temperature.argtypes = [vp, fp]
@@ -241,6 +243,11 @@ class Solver:
 
     def field_to_device(self, kind, dev_ptr):
         _check(self.lib.fvm_field_to_device(self.h, int(kind), C.c_void_p(dev_ptr)))
+
+    def colormap_to_device(self, kind, colormap, min_val, max_val, dev_ptr, fmt=0):
+        """RGBA image of a derived field into a device buffer (fmt 0: float4, 1: uchar4 per cell)."""
+        _check(self.lib.fvm_colormap_to_device(self.h, int(kind), int(colormap), float(min_val), float(max_val),
+                                               C.c_void_p(dev_ptr), int(fmt)))
 
     def cell_types_to_device(self, dev_ptr):
         _check(self.lib.fvm_cell_types_to_device(self.h, C.c_void_p(dev_ptr)))
@@ -466,6 +473,22 @@ class Server:
         st = ServerStats()
         _check(self.lib.fvm_server_get_stats(self.h, C.byref(st)))
         return st
+
+
+def colormap_table(colormap):
+    """(256, 3) float32 colour table of a colormap (fvm_colormap_table)."""
+    out = np.empty((256, 3), np.float32)
+    _check(load_library().fvm_colormap_table(int(colormap), C.c_void_p(out.ctypes.data)))
+    return out
+
+
+def write_ppm(path, rgba):
+    """Write an (ny, nx, 4) uint8 image (row 0 = bottom grid row) as a binary
+    PPM with the top row first."""
+    img = np.ascontiguousarray(np.asarray(rgba, np.uint8)[::-1, :, :3])
+    with open(path, "wb") as f:
+        f.write(b"P6\n%d %d\n255\n" % (img.shape[1], img.shape[0]))
+        f.write(img.tobytes())
 
 
 def shedding_stats(t, cd, cl, ref_length, u_inf):

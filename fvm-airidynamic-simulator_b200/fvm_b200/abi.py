@@ -17,6 +17,8 @@ FLUX_HLLC, FLUX_AUSM_PLUS = 0, 1
 LIMITER_MINMOD, LIMITER_VAN_LEER = 0, 1
 DT_FIXED, DT_RECOMPUTE = 0, 1
 FIELD_TEMPERATURE, FIELD_PRESSURE, FIELD_DENSITY, FIELD_VELOCITY_MAG, FIELD_MACH = range(5)
+CMAP_JET, CMAP_HOT, CMAP_PLASMA, CMAP_INFERNO, CMAP_VIRIDIS = range(5)
+RGBA_F32, RGBA_U8 = 0, 1
 
 STATUS = {0: "OK", 1: "INVALID", 2: "CUDA", 3: "ALLOC", 4: "STATE", 5: "TIMEOUT",
           6: "NONFINITE", 7: "BUDGET", 8: "UNSUPPORTED"}

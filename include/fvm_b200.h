@@ -335,6 +335,27 @@ int fvm_server_destroy(fvm_server *s);
 int fvm_state_max_noalloc(const float *state, int nx, int ny, size_t pitch, size_t plane, int what, float *out,
                           void *stream);
 
+/* ------------------------------------------------------------ colour images
+ * Headless form of the renderer's field pass (src/renderer.cpp:47-77 and the
+ * colour tables of src/renderer.cpp:672-799, enum ColormapType of
+ * src/include/renderer.h:14-21): one RGBA pixel per cell, row j of the image
+ * = grid row j (bottom row first, as the reference uploads its texture).
+ * SOLID and GHOST cells are dark grey (0.3); other cells show the derived
+ * field `field_kind` (enum fvm_field_kind) normalised by
+ * (v - min_val) / (max_val - min_val + 1e-4), clamped to [0, 1], looked up in
+ * the table as a linearly filtered, edge-clamped 1-D texture would.  No
+ * graphics API is involved. */
+enum fvm_colormap { FVM_CMAP_JET = 0, FVM_CMAP_HOT = 1, FVM_CMAP_PLASMA = 2, FVM_CMAP_INFERNO = 3, FVM_CMAP_VIRIDIS = 4 };
+enum fvm_pixel_format {
+    FVM_RGBA_F32 = 0,  /* 4 floats per pixel in [0, 1] */
+    FVM_RGBA_U8 = 1    /* 4 bytes per pixel, round(clamp(c) * 255) */
+};
+/* Image into a device buffer of nx*ny pixels (enqueued on the handle's stream). */
+int fvm_colormap_to_device(fvm_handle *h, int field_kind, int colormap, float min_val, float max_val,
+                           void *dev_rgba, int format);
+/* The 256-entry RGB table of a colormap (768 floats, host). */
+int fvm_colormap_table(int colormap, float *rgb_out);
+
 /* ------------------------------------------------------------ analysis
  * Vortex-shedding statistics of a force-coefficient history (samples at
  * strictly increasing times t; cd, cl from fvm_diagnostics), for the

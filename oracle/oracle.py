@@ -39,6 +39,10 @@ def _lib(bits):
     lib.orc_set_threads.argtypes = [i]
     lib.orc_set_threads.restype = i
     lib.orc_set_params.argtypes = [vp, C.POINTER(SimParams), C.POINTER(Ext)]
+    lib.orc_colormap_table.argtypes = [i, C.c_void_p]
+    lib.orc_colormap_table.restype = None
+    lib.orc_colormap.argtypes = [C.c_void_p, C.c_void_p, C.c_long, i, C.c_float, C.c_float, i, C.c_void_p]
+    lib.orc_colormap.restype = None
     lib.orc_reset.argtypes = [vp]
     lib.orc_set_geometry.argtypes = [vp, C.c_void_p, C.c_void_p]
     lib.orc_reinit.argtypes = [vp]
@@ -172,3 +176,21 @@ class Oracle:
                 dt = self.compute_dt()
             self.step(dt)
         return dt
+
+
+def colormap_table(cmap):
+    """(256, 3) float32 colour table of the renderer's colormap `cmap`."""
+    out = np.empty((256, 3), np.float32)
+    _lib(32).orc_colormap_table(int(cmap), out.ctypes.data)
+    return out
+
+
+def colormap(field, ct, cmap, lo, hi, fmt=0):
+    """Field fragment shader on the CPU: field (float32) and ct (uint8) of the
+    same shape -> (..., 4) float32 (fmt 0) or uint8 (fmt 1) RGBA."""
+    f = np.ascontiguousarray(field, np.float32)
+    c = np.ascontiguousarray(ct, np.uint8)
+    out = np.empty(f.shape + (4,), np.float32 if fmt == 0 else np.uint8)
+    _lib(32).orc_colormap(f.ctypes.data, c.ctypes.data, f.size, int(cmap), float(lo), float(hi), int(fmt),
+                          out.ctypes.data)
+    return out

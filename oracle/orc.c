@@ -1261,3 +1261,75 @@ double orc_shock_standoff(orc_solver *s) {
     }
     return NAN;
 }
+
+
+/* ------------------------------------------------------------ colour images
+ * Renderer::generate{Jet,Hot,Plasma,Inferno,Viridis}Colormap
+ * (src/renderer.cpp:672-716, 719-734, 737-754, 757-779, 782-799), t = i/255. */
+static float clampf01(float x, float lo, float hi) { return x < lo ? lo : (x > hi ? hi : x); }
+
+void orc_colormap_table(int cmap, float rgb[768]) {
+    for (int i = 0; i < 256; i++) {
+        const float t = (float)i / 255.0f;
+        float c[3];
+        if (cmap == 0) { /* jet: five linear pieces */
+            if (t < 0.125f) { c[0] = 0.0f; c[1] = 0.0f; c[2] = 0.5f + 4.0f * t; }
+            else if (t < 0.375f) { c[0] = 0.0f; c[1] = 4.0f * (t - 0.125f); c[2] = 1.0f; }
+            else if (t < 0.625f) { c[0] = 4.0f * (t - 0.375f); c[1] = 1.0f; c[2] = 1.0f - 4.0f * (t - 0.375f); }
+            else if (t < 0.875f) { c[0] = 1.0f; c[1] = 1.0f - 4.0f * (t - 0.625f); c[2] = 0.0f; }
+            else { c[0] = 1.0f - 4.0f * (t - 0.875f); c[1] = 0.0f; c[2] = 0.0f; }
+        } else if (cmap == 1) { /* hot */
+            c[0] = t * 2.5f < 1.0f ? t * 2.5f : 1.0f;
+            c[1] = clampf01((t - 0.4f) * 2.5f, 0.0f, 1.0f);
+            c[2] = (t - 0.8f) * 5.0f > 0.0f ? (t - 0.8f) * 5.0f : 0.0f;
+        } else if (cmap == 2) { /* plasma: cubic / quartic fits */
+            c[0] = 0.050383f + t * (2.028462f + t * (-1.312035f + t * 0.233106f));
+            c[1] = 0.029803f + t * (0.192182f + t * (1.429032f + t * (-1.651143f + t * 0.500000f)));
+            c[2] = 0.527975f + t * (1.573141f + t * (-2.481592f + t * 0.880392f));
+            for (int k = 0; k < 3; k++) c[k] = clampf01(c[k], 0.0f, 1.0f);
+        } else if (cmap == 3) { /* inferno: the generator's final (linear) form */
+            c[0] = clampf01(1.5f * t, 0.0f, 1.0f);
+            c[1] = clampf01(2.0f * (t - 0.25f), 0.0f, 1.0f);
+            c[2] = clampf01(0.6f - 1.2f * t, 0.0f, 0.6f);
+        } else { /* viridis: cubic fits */
+            c[0] = 0.267004f + t * (0.003991f + t * (0.494266f + t * 0.234652f));
+            c[1] = 0.004874f + t * (1.014627f + t * (-0.531556f + t * 0.512042f));
+            c[2] = 0.329415f + t * (1.423671f + t * (-2.252694f + t * 0.499477f));
+            for (int k = 0; k < 3; k++) c[k] = clampf01(c[k], 0.0f, 1.0f);
+        }
+        for (int k = 0; k < 3; k++) rgb[3 * i + k] = c[k];
+    }
+}
+
+/* FIELD_FRAGMENT_SHADER (src/renderer.cpp:47-77) per cell: classes 1 and 2
+ * (cellType in (0.5, 2.5)) grey 0.3; otherwise clamp((v-lo)/(hi-lo+1e-4)),
+ * then the OpenGL LINEAR / CLAMP_TO_EDGE lookup of a 256-texel 1-D texture:
+ * u = s*256 - 1/2, texels floor(u) and floor(u)+1 clamped to [0,255],
+ * weights 1-frac(u), frac(u).  RGBA8 = round-to-nearest(c*255). */
+void orc_colormap(const float *field, const uint8_t *ct, long n, int cmap, float lo, float hi, int fmt, void *out) {
+    float tab[768];
+    orc_colormap_table(cmap, tab);
+    for (long e = 0; e < n; e++) {
+        float c[3];
+        if (ct[e] == 1 || ct[e] == 2) {
+            c[0] = c[1] = c[2] = 0.3f;
+        } else {
+            float sn = clampf01((field[e] - lo) / (hi - lo + 0.0001f), 0.0f, 1.0f);
+            float u = sn * 256.0f - 0.5f;
+            float fl = floorf(u);
+            float w = u - fl;
+            int a = (int)fl, b = (int)fl + 1;
+            a = a < 0 ? 0 : (a > 255 ? 255 : a);
+            b = b < 0 ? 0 : (b > 255 ? 255 : b);
+            for (int k = 0; k < 3; k++) c[k] = (1.0f - w) * tab[3 * a + k] + w * tab[3 * b + k];
+        }
+        if (fmt == 0) {
+            float *o = (float *)out + 4 * e;
+            o[0] = c[0]; o[1] = c[1]; o[2] = c[2]; o[3] = 1.0f;
+        } else {
+            uint8_t *o = (uint8_t *)out + 4 * e;
+            for (int k = 0; k < 3; k++) o[k] = (uint8_t)nearbyintf(clampf01(c[k], 0.0f, 1.0f) * 255.0f);
+            o[3] = 255;
+        }
+    }
+}

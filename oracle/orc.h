@@ -77,6 +77,14 @@ void orc_stage1(orc_solver *s, double dt, int with_ghost, double *out5[5]);
 void orc_diagnostics(orc_solver *s, fvm_diag *out);
 double orc_shock_standoff(orc_solver *s);
 
+/* Colour images (test infrastructure for fvm_colormap_to_device): the
+ * renderer's 256-entry colour tables (src/renderer.cpp:672-799) and the field
+ * fragment shader (src/renderer.cpp:47-77) restated on the CPU in float.
+ * field: n derived values; ct: n cell classes; fmt 0 -> n*4 floats,
+ * fmt 1 -> n*4 bytes. */
+void orc_colormap_table(int cmap, float rgb[768]);
+void orc_colormap(const float *field, const uint8_t *ct, long n, int cmap, float lo, float hi, int fmt, void *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,81 @@
+"""Colour images (fvm_colormap_*): the renderer's colour tables (CPU) and the
+field pass on the GPU against the oracle's CPU restatement of the fragment
+shader on the same derived field."""
+import numpy as np
+import pytest
+
+from helpers import small
+import fvm_b200
+from fvm_b200 import abi
+from oracle import oracle
+
+
+@pytest.mark.parametrize("cmap", range(5))
+def test_library_tables_equal_the_oracle_tables(cmap):
+    assert np.array_equal(fvm_b200.colormap_table(cmap), oracle.colormap_table(cmap))
+
+
+def test_table_end_points():
+    jet, hot = fvm_b200.colormap_table(abi.CMAP_JET), fvm_b200.colormap_table(abi.CMAP_HOT)
+    assert tuple(jet[0]) == (0.0, 0.0, 0.5) and tuple(jet[255]) == (0.5, 0.0, 0.0)
+    assert tuple(hot[0]) == (0.0, 0.0, 0.0) and np.allclose(hot[255], 1.0, atol=1e-6)
+    for c in range(5):
+        t = fvm_b200.colormap_table(c)
+        assert t.min() >= 0.0 and t.max() <= 1.0
+
+
+def test_oracle_shader_masks_walls_and_clamps():
+    field = np.array([[-1.0, 0.0, 0.5, 2.0, 3.0, 0.5]], np.float32)
+    ct = np.array([[0, 0, 0, 0, 0, 1]], np.uint8)
+    img = oracle.colormap(field, ct, abi.CMAP_HOT, 0.0, 1.0, fmt=0)
+    assert np.allclose(img[0, 5], (0.3, 0.3, 0.3, 1.0))
+    assert np.array_equal(img[0, 0], img[0, 1])  # below range clamps to the first texel
+    assert np.array_equal(img[0, 3], img[0, 4])  # above range clamps to the last texel
+    assert np.allclose(img[0, 3, :3], oracle.colormap_table(abi.CMAP_HOT)[255])
+    u8 = oracle.colormap(field, ct, abi.CMAP_HOT, 0.0, 1.0, fmt=1)
+    assert u8.dtype == np.uint8 and (u8[..., 3] == 255).all()
+
+
+def test_errors_and_ppm(tmp_path):
+    with pytest.raises(fvm_b200.FvmError):
+        fvm_b200.colormap_table(7)
+    img = np.zeros((3, 5, 4), np.uint8)
+    img[0, :, 0] = 255  # bottom row red
+    path = tmp_path / "f.ppm"
+    fvm_b200.write_ppm(path, img)
+    data = path.read_bytes()
+    assert data.startswith(b"P6\n5 3\n255\n") and len(data) == len(b"P6\n5 3\n255\n") + 45
+    assert data[-15] == 255  # last row written is the bottom grid row
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", [abi.FIELD_TEMPERATURE, abi.FIELD_MACH, abi.FIELD_PRESSURE])
+def test_gpu_image_matches_oracle_shader(kind):
+    import torch
+    p, e = small("euler_m3_circle", 320, 160)
+    s = fvm_b200.Solver(p, e)
+    p.dt = s.compute_dt()
+    s.step(60)
+    n = p.nx * p.ny
+    field = torch.empty(n, dtype=torch.float32, device="cuda")
+    s.field_to_device(kind, field.data_ptr())
+    s.synchronize()
+    f = field.cpu().numpy().reshape(p.ny, p.nx)
+    ct = s.cell_types().reshape(p.ny, p.nx)
+    fluid = (ct != abi.CELL_SOLID) & (ct != abi.CELL_GHOST)
+    lo, hi = float(f[fluid].min()), float(f[fluid].max())
+    for cmap in range(5):
+        rgba = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+        s.colormap_to_device(kind, cmap, lo, hi, rgba.data_ptr(), abi.RGBA_F32)
+        u8 = torch.empty((n, 4), dtype=torch.uint8, device="cuda")
+        s.colormap_to_device(kind, cmap, lo, hi, u8.data_ptr(), abi.RGBA_U8)
+        s.synchronize()
+        g32 = rgba.cpu().numpy().reshape(p.ny, p.nx, 4)
+        g8 = u8.cpu().numpy().reshape(p.ny, p.nx, 4)
+        r32 = oracle.colormap(f, ct, cmap, lo, hi, fmt=0)
+        r8 = oracle.colormap(f, ct, cmap, lo, hi, fmt=1)
+        # float: the GPU's normalising division is the fast approximate one
+        assert np.abs(g32 - r32).max() <= 2e-5, cmap
+        d8 = np.abs(g8.astype(int) - r8.astype(int))
+        assert d8.max() <= 1 and (d8 > 0).mean() <= 1e-3, cmap
+        assert np.array_equal(g8[~fluid], r8[~fluid])

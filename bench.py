@@ -542,6 +542,19 @@ def main():
         ktimes = s.kernel_times()
         s.set_kernel_timing(False)
 
+        # ---- colour image of the Mach field (headless renderer pass), RGBA8
+        img = torch.empty((nx * ny, 4), dtype=torch.uint8, device="cuda")
+        for _ in range(3):
+            s.colormap_to_device(abi.FIELD_MACH, abi.CMAP_JET, 0.0, 10.0, img.data_ptr(), abi.RGBA_U8)
+        c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        c0.record(stream)
+        for _ in range(10):
+            s.colormap_to_device(abi.FIELD_MACH, abi.CMAP_JET, 0.0, 10.0, img.data_ptr(), abi.RGBA_U8)
+        c1.record(stream)
+        torch.cuda.synchronize()
+        cmap_ms = c0.elapsed_time(c1) / 10
+        del img
+
         # ---- end to end through the C ABI with host buffers: upload state,
         # K steps, download state
         import ctypes as C
@@ -606,6 +619,10 @@ def main():
                     "h2d_bytes_per_step": cells * 20 / args.steps, "d2h_bytes_per_step": cells * 20 / args.steps},
             "gpu_launches": launches,
             "clocks": clk,
+            # Mach field (reads rho, rho_u, rho_v, rho_e = 16 B + class 1 B, writes 4 B per cell)
+            "colormap": {"field": "mach", "format": "rgba8", "ms_per_image": cmap_ms,
+                         "gbs": 21 * cells / (cmap_ms / 1e3) / 1e9,
+                         "frac": 21 * cells / (cmap_ms / 1e3) / 1e9 / hbm},
             **extras,
         }
         print(json.dumps(line), flush=True)

@@ -33,7 +33,8 @@ EXPORTS = [
     "fvm_batch_read_fields", "fvm_batch_diagnostics", "fvm_batch_memory_usage", "fvm_batch_launch_count",
     "fvm_batch_instance_bytes", "fvm_batch_retire", "fvm_batch_trim", "fvm_server_create", "fvm_server_submit",
     "fvm_server_poll", "fvm_server_wait", "fvm_server_drain", "fvm_server_get_stats", "fvm_server_destroy",
-    "fvm_state_max_noalloc", "fvm_shedding_stats", "fvm_colormap_to_device", "fvm_colormap_table", "fvm_autotune", "fvm_get_tune", "fvm_debug_stage1", "fvm_debug_ghost_table", "fvm_build_info",
+    "fvm_state_max_noalloc", "fvm_shedding_stats", "fvm_colormap_to_device", "fvm_colormap_table",
+    "fvm_save_checkpoint", "fvm_load_checkpoint", "fvm_checkpoint_info", "fvm_autotune", "fvm_get_tune", "fvm_debug_stage1", "fvm_debug_ghost_table", "fvm_build_info",
 ]
 
 
@@ -88,6 +89,9 @@ def load_library(path=None):
     lib.fvm_field_to_device.argtypes = [vp, i, vp]
     lib.fvm_colormap_to_device.argtypes = [vp, i, i, f, f, vp, i]
     lib.fvm_colormap_table.argtypes = [i, vp]
+    lib.fvm_save_checkpoint.argtypes = [vp, Pp, C.c_char_p]
+    lib.fvm_load_checkpoint.argtypes = [vp, C.c_char_p, Pp]
+    lib.fvm_checkpoint_info.argtypes = [C.c_char_p, Pp, C.POINTER(Ext)]
     lib.fvm_cell_types_to_device.argtypes = [vp, vp]
     lib.fvm_vector_arrows.argtypes = [vp, vp, i, i, f, f, f, f, C.POINTER(i)]
     lib.fvm_max_temperature.argtypes = [vp, fp]
@@ -243,6 +247,17 @@ class Solver:
 
     def field_to_device(self, kind, dev_ptr):
         _check(self.lib.fvm_field_to_device(self.h, int(kind), C.c_void_p(dev_ptr)))
+
+    def save_checkpoint(self, path):
+        """Write the solve (state, parameters, time-step state) to a checkpoint file."""
+        _check(self.lib.fvm_save_checkpoint(self.h, C.byref(self.params), os.fsencode(path)))
+
+    def load_checkpoint(self, path):
+        """Restore a checkpoint into this handle; returns (and adopts) the saved parameters."""
+        p = SimParams()
+        _check(self.lib.fvm_load_checkpoint(self.h, os.fsencode(path), C.byref(p)))
+        self.params = p
+        return p
 
     def colormap_to_device(self, kind, colormap, min_val, max_val, dev_ptr, fmt=0):
         """RGBA image of a derived field into a device buffer (fmt 0: float4, 1: uchar4 per cell)."""
@@ -475,6 +490,41 @@ class Server:
         return st
 
 
+CHECKPOINT_MAGIC = b"FVMB200C"
+
+
+def read_checkpoint(path):
+    """Read a checkpoint file without a GPU: (header dict, fields (5, ny, nx)
+    float32).  The header dict holds the saved SimParams / Ext and the
+    time-step state; the payload CRC-32 is verified."""
+    import struct
+    import zlib
+    with open(path, "rb") as f:
+        head = f.read(256)
+        if len(head) != 256 or head[:8] != CHECKPOINT_MAGIC:
+            raise FvmError(1, f"{path}: not a checkpoint file")
+        version, hbytes, nx, ny, nf, flags = struct.unpack_from("<IIiiII", head, 8)
+        next_dt, t_dev, cfl_speed, cfl_nu = struct.unpack_from("<ffff", head, 32)
+        payload_bytes, crc = struct.unpack_from("<QI", head, 48)
+        if version != 1 or hbytes != 256 or nf != 5 or payload_bytes != nx * ny * 20:
+            raise FvmError(8, f"{path}: unsupported checkpoint layout")
+        params = SimParams.from_buffer_copy(head, 64)
+        ext = Ext.from_buffer_copy(head, 64 + C.sizeof(SimParams))
+        data = f.read(payload_bytes)
+    if len(data) != payload_bytes or zlib.crc32(data) != crc:
+        raise FvmError(1, f"{path}: payload truncated or checksum mismatch")
+    fields = np.frombuffer(data, np.float32).reshape(5, ny, nx).copy()
+    return {"params": params, "ext": ext, "next_dt": next_dt, "t_device": t_dev, "flags": flags,
+            "cfl": (cfl_speed, cfl_nu)}, fields
+
+
+def checkpoint_info(path):
+    """Validate a checkpoint file in the library (no device needed): (SimParams, Ext)."""
+    p, e = SimParams(), Ext()
+    _check(load_library().fvm_checkpoint_info(os.fsencode(path), C.byref(p), C.byref(e)))
+    return p, e
+
+
 def colormap_table(colormap):
     """(256, 3) float32 colour table of a colormap (fvm_colormap_table)."""
     out = np.empty((256, 3), np.float32)
@@ -515,5 +565,5 @@ def gpu_mem_info():
     return f.value, t.value
 
 
-__all__ = ["Solver", "Batch", "Server", "shedding_stats", "instance_bytes", "FvmError", "SimParams", "Ext", "Diag", "params_default", "compute_derived",
+__all__ = ["Solver", "Batch", "Server", "shedding_stats", "read_checkpoint", "write_ppm", "colormap_table", "instance_bytes", "FvmError", "SimParams", "Ext", "Diag", "params_default", "compute_derived",
            "ext_default", "workload", "load_library", "gpu_mem_info", "EXPORTS", "LIB_PATH"]

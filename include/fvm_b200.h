@@ -356,6 +356,22 @@ int fvm_colormap_to_device(fvm_handle *h, int field_kind, int colormap, float mi
 /* The 256-entry RGB table of a colormap (768 floats, host). */
 int fvm_colormap_table(int colormap, float *rgb_out);
 
+/* ------------------------------------------------------------ checkpoints
+ * Save / restore a solve to a file: a 256-byte header (magic "FVMB200C",
+ * version 1, grid, the solve's parameters and extension knobs, the next
+ * step's dt, the device simulated time and the last step's CFL maxima) and
+ * the five conserved fields as nx*ny float32 planes (fvm_read_fields layout),
+ * with a CRC-32 of the fields in the header.  Loading re-initialises the
+ * handle from the saved parameters and continues bit for bit where the saved
+ * solve would have.  No reference counterpart (the reference has no
+ * checkpoints). */
+int fvm_save_checkpoint(fvm_handle *h, const fvm_sim_params *p, const char *path);
+/* *p_out (may be NULL) receives the saved parameters (t_current, step, dt). */
+int fvm_load_checkpoint(fvm_handle *h, const char *path, fvm_sim_params *p_out);
+/* Validate a checkpoint file (header and checksum) without a handle or a
+ * device; *p_out / *ext_out (may be NULL) receive its parameters. */
+int fvm_checkpoint_info(const char *path, fvm_sim_params *p_out, fvm_ext *ext_out);
+
 /* ------------------------------------------------------------ analysis
  * Vortex-shedding statistics of a force-coefficient history (samples at
  * strictly increasing times t; cd, cl from fvm_diagnostics), for the

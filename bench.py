@@ -43,6 +43,8 @@ WORKLOADS = {
     # many-solve workloads (own code paths below)
     "batched_uneven": (0, 0),
     "serving": (0, 0),
+    # the stated runs of the three single-solve configurations and their outputs
+    "config_outputs": (0, 0),
 }
 BATCH_SEED, SERVE_SEED = 4, 5
 # Algorithmic HBM bytes per cell for each launch of the step (5 conserved
@@ -380,6 +382,81 @@ def run_reference_arm(args, params, ext, ws, rank, dist):
     print(json.dumps(line), flush=True)
 
 
+def run_config_outputs(args, ws, rank, local):
+    """The stated runs and outputs of the single-solve configurations, each
+    timed on the device: Euler Mach-3 circle 512x256 for 200 steps (AUSM+ and
+    HLLC); Re-200 vortex street 2048x1024 for 20000 steps (drag / lift
+    history, Strouhal number when the history holds whole shedding cycles);
+    Mach-8 blunted cone 8192x4096 for 2000 steps (standoff, wall heat flux)."""
+    import torch
+    import fvm_b200
+    torch.cuda.set_device(local)
+    out = {}
+
+    def timed(s, n, every=None, sample=None):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        total = 0.0
+        done = 0
+        while done < n:
+            k = min(every or n, n - done)
+            e0.record()
+            s.step(k)
+            e1.record()
+            torch.cuda.synchronize()
+            total += e0.elapsed_time(e1)
+            done += k
+            if sample:
+                sample(s)
+        return total
+
+    for flux, tag in ((abi.FLUX_AUSM_PLUS, "ausm+"), (abi.FLUX_HLLC, "hllc")):
+        p, e = abi.workload("euler_m3_circle", 512, 256)
+        e.flux_scheme, e.dt_policy = flux, abi.DT_RECOMPUTE
+        s = fvm_b200.Solver(p, e)
+        ms = timed(s, 200)
+        d = s.diagnostics()
+        out[f"c1_euler_m3_circle_512x256_200steps_{tag}"] = {
+            "ms_total": ms, "cell_updates_per_s": 512 * 256 * 200 / (ms / 1e3), "cd": d.cd, "cl": d.cl,
+            "mass": d.mass, "t_end_s": s.params.t_current}
+        s.close()
+    p, e = abi.workload("ns_karman_re200", 2048, 1024)
+    e.dt_policy = abi.DT_RECOMPUTE
+    s = fvm_b200.Solver(p, e)
+    hist = []
+    ms = timed(s, 20000, every=20, sample=lambda x: hist.append((x.params.t_current, x.diagnostics())))
+    t = np.array([h[0] for h in hist])
+    cd = np.array([h[1].cd for h in hist])
+    cl = np.array([h[1].cl for h in hist])
+    D, U = e.ref_length, p.u_inf
+    c2 = {"ms_total": ms, "cell_updates_per_s": 2048 * 1024 * 20000 / (ms / 1e3),
+          "t_end_over_D_per_U": float(t[-1] / (D / U)), "cd_final": float(cd[-1]), "cl_final": float(cl[-1]),
+          "cd_mean_last_quarter": float(cd[3 * len(cd) // 4:].mean())}
+    try:
+        st = fvm_b200.shedding_stats(t[len(t) // 2:], cd[len(t) // 2:], cl[len(t) // 2:], D, U)
+        c2.update({"strouhal": st.strouhal, "cd_cycle_mean": st.cd_mean, "shedding_cycles": st.cycles})
+    except fvm_b200.FvmError:
+        c2["strouhal"] = None  # no whole shedding cycle yet in the stated 20000 steps
+    out["c2_ns_karman_re200_2048x1024_20000steps"] = c2
+    s.close()
+    p, e = abi.workload("ns_hypersonic_cone", 8192, 4096)
+    e.dt_policy = abi.DT_RECOMPUTE
+    s = fvm_b200.Solver(p, e)
+    ms = timed(s, 2000)
+    d = s.diagnostics()
+    out["c3_ns_hypersonic_cone_8192x4096_2000steps"] = {
+        "ms_total": ms, "cell_updates_per_s": 8192 * 4096 * 2000 / (ms / 1e3), "standoff_m": s.shock_standoff(),
+        "standoff_over_nose_radius": s.shock_standoff() / p.obstacle_r, "wall_heat_w_per_m": d.wall_heat,
+        "wall_heat_max_w_per_m2": d.wall_heat_max, "cd": d.cd, "t_end_s": s.params.t_current}
+    s.close()
+    if rank == 0:
+        c3 = out["c3_ns_hypersonic_cone_8192x4096_2000steps"]
+        print(json.dumps({"metric": "cell_updates_per_s", "value": c3["cell_updates_per_s"] * ws,
+                          "unit": "cell-updates/s", "n_gpus": ws, "steps": 2000, "warmup": 0,
+                          "ms_per_step": c3["ms_total"] / 2000, "higher_is_better": True, "scaling": "weak",
+                          "vs_baseline": None, "dtype": "f32", "data": "synthetic (freestream start)",
+                          "config": {"workload": "config_outputs"}, "outputs": out}), flush=True)
+
+
 def run_many_solves(args, ws, rank, local, dist):
     """batched_uneven / serving: one line per run on rank 0 (other ranks run
     replicas of the same work; weak scaling)."""
@@ -486,14 +563,21 @@ def main():
     assert args.warmup >= 3, "at least 3 warm-up steps"
 
     ws, rank, local, dist = dist_setup()
+    if args.workload == "config_outputs" and args.impl == "fvm":
+        run_config_outputs(args, ws, rank, local)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
     if args.workload in ("batched_uneven", "serving"):
         run_many_solves(args, ws, rank, local, dist)
         if dist is not None:
             dist.destroy_process_group()
         return
-    nx, ny = WORKLOADS[args.workload]
+    # the reference arm of config_outputs times the cone case's CPU restatement
+    wl = "ns_hypersonic_cone" if args.workload == "config_outputs" else args.workload
+    nx, ny = WORKLOADS[wl]
     nx, ny = args.nx or nx, args.ny or ny
-    params, ext = abi.workload(args.workload, nx, ny)
+    params, ext = abi.workload(wl, nx, ny)
 
     if args.impl == "reference":
         run_reference_arm(args, params, ext, ws, rank, dist)

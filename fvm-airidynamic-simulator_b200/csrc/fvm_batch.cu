@@ -20,6 +20,7 @@
 struct fvm_batch {
     cudaStream_t own = nullptr;
     cudaStream_t stream = nullptr;
+    cudaStream_t admit = nullptr;     // set-up of instances being added (overlaps running steps)
     fvm_ext ext{};
     StageTune tune{128, 6, 32};
     bool tune_fixed = false;          // FVM_BATCH_TUNE pins the launch shape
@@ -185,7 +186,9 @@ extern "C" int fvm_batch_create(fvm_batch **out, const fvm_ext *ext) {
         b->ext = *ext;
     else
         fvm_ext_default(&b->ext);
-    if (cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking) != cudaSuccess) {
+    if (cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->admit, cudaStreamNonBlocking) != cudaSuccess) {
+        if (b->own) cudaStreamDestroy(b->own);
         delete b;
         return berr(FVM_ERR_CUDA, "stream creation failed");
     }
@@ -213,6 +216,7 @@ extern "C" int fvm_batch_destroy(fvm_batch *b) {
     cudaFree(b->d_visc_tiles);
     cudaFree(b->d_chunks);
     if (b->own) cudaStreamDestroy(b->own);
+    if (b->admit) cudaStreamDestroy(b->admit);
     delete b;
     return FVM_OK;
 }
@@ -239,12 +243,16 @@ extern "C" size_t fvm_batch_instance_bytes(int nx, int ny) {
 extern "C" int fvm_batch_add(fvm_batch *b, const fvm_sim_params *p, int *id_out) {
     CHECK_BATCH(b);
     if (!p || !id_out) return berr(FVM_ERR_INVALID, "null argument");
+    // The instance is set up on the admission stream, so adding does not wait
+    // for batched steps already queued on the batch stream (the new instance
+    // joins the tile list at the next fvm_batch_step).
     fvm_handle *h = nullptr;
     // a retired instance of the same grid size keeps its buffers: reset it in place
     for (size_t k = 0; k < b->parked.size(); k++) {
         fvm_handle *c = b->parked[k];
         if (c->g.nx == p->nx && c->g.ny == p->ny) {
             b->parked.erase(b->parked.begin() + (long)k);
+            c->stream = b->admit;  // parked: no work of its own pending
             if (int r = fvm_reset(c, p)) {
                 fvm_destroy(c);
                 return r;
@@ -255,7 +263,7 @@ extern "C" int fvm_batch_add(fvm_batch *b, const fvm_sim_params *p, int *id_out)
     }
     if (!h) {
         if (int r = fvm_create(&h)) return r;
-        fvm_set_stream(h, b->stream);
+        h->stream = b->admit;
         if (int r = fvm_initialize(h, p, &b->ext)) {
             fvm_destroy(h);
             return r;
@@ -278,18 +286,18 @@ extern "C" int fvm_batch_add(fvm_batch *b, const fvm_sim_params *p, int *id_out)
             return r;
         }
     }
-    // device scalars of the fresh solve, written on the batch stream (which
-    // does not synchronise with the legacy default stream)
+    // device scalars of the fresh solve
     DevScalars init;
-    BCK(cudaMemcpyAsync(&init, h->sc, sizeof init, cudaMemcpyDeviceToHost, b->stream));
-    BCK(cudaStreamSynchronize(b->stream));
+    BCK(cudaMemcpyAsync(&init, h->sc, sizeof init, cudaMemcpyDeviceToHost, b->admit));
+    BCK(cudaStreamSynchronize(b->admit));
     init.dt = dt;
     init.t = p->t_current;
     init.parity = 0;
     init.counter = 0;
     init.red[0] = init.red[1] = 0.0f;
-    BCK(cudaMemcpyAsync(h->sc, &init, sizeof init, cudaMemcpyHostToDevice, b->stream));
-    BCK(cudaStreamSynchronize(b->stream));
+    BCK(cudaMemcpyAsync(h->sc, &init, sizeof init, cudaMemcpyHostToDevice, b->admit));
+    BCK(cudaStreamSynchronize(b->admit));
+    h->stream = b->stream;
     int id = -1;
     for (size_t k = 0; k < b->slots.size(); k++)
         if (!b->slots[k]) {

@@ -10,7 +10,9 @@
 //   2. advance every admitted solve by k batched steps, k = the fewest steps
 //      any admitted solve still needs, capped by the chunk size -- so at least
 //      one solve finishes at every chunk end and new arrivals wait at most one
-//      chunk;
+//      chunk.  The chunk is queued asynchronously; requests that arrive while
+//      it runs are admitted (their set-up runs on the batch's admission
+//      stream, overlapping the chunk) and join at the next chunk;
 //   3. retire the solves that reached their step count: final state to the
 //      caller's arrays, diagnostics into the result, instance parked for reuse.
 // Retired instances keep their device memory and are reset in place when a
@@ -170,6 +172,7 @@ static void worker_main(fvm_server *s) {
             k = std::min(k, r.steps - r.done);
             cells += (double)r.p.nx * r.p.ny;
         }
+        const size_t stepping = s->active.size();  // solves in this chunk
         lk.unlock();
         int rc = FVM_OK;
         float ms = 0.0f;
@@ -177,6 +180,12 @@ static void worker_main(fvm_server *s) {
             cudaEventRecord(s->ev0, s->stream);
             rc = fvm_batch_step(s->b, k);
             cudaEventRecord(s->ev1, s->stream);
+        }
+        lk.lock();
+        // admit arrivals while the chunk runs; they join at the next chunk
+        if (rc == FVM_OK) admit(s, lk);
+        lk.unlock();
+        if (k > 0) {
             if (rc == FVM_OK) rc = fvm_batch_synchronize(s->b);
             if (rc == FVM_OK && cudaEventElapsedTime(&ms, s->ev0, s->ev1) != cudaSuccess) ms = 0.0f;
         }
@@ -187,9 +196,15 @@ static void worker_main(fvm_server *s) {
             s->cell_updates += cells * k;
             s->step_ms.insert(s->step_ms.end(), (size_t)k, ms / k);
         }
-        // retire finished solves (all of them if the chunk failed)
+        // retire finished solves (all of them if the chunk failed); solves
+        // admitted during the chunk (index >= stepping) did not step
         std::vector<Request> keep;
-        for (Request &r : s->active) {
+        for (size_t idx = 0; idx < s->active.size(); idx++) {
+            Request &r = s->active[idx];
+            if (idx >= stepping && rc == FVM_OK) {
+                keep.push_back(r);
+                continue;
+            }
             if (rc == FVM_OK) r.done += k;
             if (rc != FVM_OK || r.done >= r.steps) {
                 lk.unlock();

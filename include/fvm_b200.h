@@ -223,7 +223,7 @@ int fvm_kernel_times(fvm_handle *h, fvm_kernel_time *out, int cap, int *count_ou
 
 /* Autotuner: times every candidate launch tuning of the marching step
  * kernels (threads per CTA 128/256, TMA ring depth 4/6 rows, rows per CTA
- * 16..256) over `steps` steps of this solve, restoring the state after each,
+ * 4..256) over `steps` steps of this solve, restoring the state after each,
  * keeps the fastest for this handle and caches it for the grid class (grid
  * size, viscous flag, flux scheme, limiter) for later handles in the process.
  * *best_ms_out receives the winner's time per step. */

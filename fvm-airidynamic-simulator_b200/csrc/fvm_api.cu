@@ -222,12 +222,11 @@ static void free_buffers(fvm_handle *h) {
     h->parity_base = nullptr;
 }
 
-// Launch tuning of the marching kernels per grid class.  Default: 128
-// threads, 6-slot ring, rows per CTA chosen so a launch spans ~6 waves of
-// the 148 SMs x ~5 resident CTAs (short enough rows to balance the last
-// wave, long enough to amortise the 4-row halo).  FVM_TUNE="nt,ring,rows"
-// overrides; fvm_autotune measures the candidates and caches the winner per
-// grid class for the process.
+// Launch tuning of the marching kernels per grid class: threads per CTA,
+// input ring depth (rows) and rows per CTA.  The default comes from
+// heuristic_tune below; FVM_TUNE="nt,ring,rows" overrides it; fvm_autotune
+// measures the candidates and caches the winner per grid class for the
+// process.
 struct TuneKey {
     int nx, ny, viscous, scheme, limiter;
     bool operator<(const TuneKey &o) const {

@@ -5,13 +5,15 @@
 // W = NT-4 output columns and `rows` output rows.  It walks the strip from
 // bottom to top.  Each incoming row (the 5 conserved planes of the input
 // state, columns [i0-4, i0+W+4)) is staged into a shared-memory ring by a 3-D
-// TMA load (x, y, field) signalled on an mbarrier, issued ahead of use.  The
-// stage kernels advance two rows per step (primitives of the incoming rows,
-// their x-faces and two y-faces, update of the two rows two behind), the
-// viscous kernel one row per step, so every face flux is computed exactly
-// once per strip and each input cell crosses HBM once (halo re-reads hit L2).  Domain-edge halos use the
-// reference's clamp-to-edge semantics (src/solver.cu:1484-1488): rows by
-// clamping the TMA row coordinate, columns by clamping the shared-memory column.
+// TMA load (x, y, field) signalled on an mbarrier, issued ahead of use.  Both
+// kernel families advance two rows per step (stage: primitives of the
+// incoming rows, their x-faces and two y-faces, update of the two rows two
+// behind; viscous: primitives, stress of the two rows one behind, update of
+// the two rows two behind), so every face flux is computed exactly once per
+// strip and each input cell crosses HBM once (halo re-reads hit L2).
+// Domain-edge halos use the reference's clamp-to-edge semantics
+// (src/solver.cu:1484-1488): rows by clamping the TMA row coordinate, columns
+// by clamping the shared-memory column.
 #include <algorithm>
 #include <cstdio>
 

@@ -198,6 +198,9 @@ static void drop_graphs(fvm_handle *h) {
         if (h->graph[k]) cudaGraphExecDestroy(h->graph[k]);
         h->graph[k] = nullptr;
         h->graph_key[k] = 0;
+        if (h->graph1[k]) cudaGraphExecDestroy(h->graph1[k]);
+        h->graph1[k] = nullptr;
+        h->graph1_key[k] = 0;
     }
 }
 
@@ -593,9 +596,14 @@ static void swap_state(fvm_handle *h) {
 // Make sc->dt hold the dt of the next step.
 static int prepare_dt(fvm_handle *h, fvm_sim_params *p) {
     if (h->ext.dt_policy == FVM_DT_FIXED) {
+        // the step kernels never change sc->dt under this policy: write it
+        // only when the caller's dt differs from the one already there
+        if (h->dt_ready && h->fixed_dt == p->dt) return FVM_OK;
         k_set_scalars<<<1, 1, 0, h->stream>>>(h->sc, p->dt, p->t_current, 0);
         CK(cudaGetLastError());
         h->launches++;
+        h->fixed_dt = p->dt;
+        h->dt_ready = true;
         return FVM_OK;
     }
     if (!h->dt_ready) {
@@ -671,7 +679,7 @@ extern "C" int fvm_steps(fvm_handle *h, fvm_sim_params *p, int n) {
         drop_graphs(h);
     }
     if (int r = prepare_dt(h, p)) return r;
-    const bool use_graph = !h->timing && n >= 2 && h->stream != nullptr && h->stream != cudaStreamLegacy &&
+    const bool use_graph = !h->timing && h->stream != nullptr && h->stream != cudaStreamLegacy &&
                            h->stream != cudaStreamPerThread && getenv("FVM_NO_GRAPH") == nullptr;
     int done = 0;
     if (use_graph && n >= 2) {
@@ -705,6 +713,34 @@ extern "C" int fvm_steps(fvm_handle *h, fvm_sim_params *p, int n) {
             CK(cudaGraphLaunch(h->graph[par], h->stream));
             h->launches += 2 * per_step;
         }
+    }
+    if (use_graph && done < n) {
+        // one remaining step: a captured single step for this buffer parity
+        if (!h->parity_base) h->parity_base = h->buf[BUF_N];
+        const int par = (h->buf[BUF_N] == h->parity_base) ? 0 : 1;
+        unsigned long long key = graph_key(h);
+        if (h->graph1[par] && h->graph1_key[par] != key) {
+            cudaGraphExecDestroy(h->graph1[par]);
+            h->graph1[par] = nullptr;
+        }
+        if (!h->graph1[par]) {
+            cudaGraph_t gr;
+            CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+            long long before = h->launches;
+            int r1 = enqueue_step(h);
+            cudaError_t ec = cudaStreamEndCapture(h->stream, &gr);
+            h->launches = before;
+            if (r1) return r1;
+            CK(ec);
+            cudaError_t ei = cudaGraphInstantiate(&h->graph1[par], gr, 0);
+            cudaGraphDestroy(gr);
+            CK(ei);
+            h->graph1_key[par] = key;
+        }
+        CK(cudaGraphLaunch(h->graph1[par], h->stream));
+        h->launches += h->prm.enable_viscosity ? 6 : 4;
+        swap_state(h);
+        done++;
     }
     for (; done < n; done++) {
         if (int r = enqueue_step(h)) return r;

@@ -169,6 +169,7 @@ extern "C" int fvm_load_checkpoint(fvm_handle *h, const char *path, fvm_sim_para
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return ckerr(FVM_ERR_CUDA, cudaGetErrorString(e));
     h->dt_ready = (hd.flags & kFlagDtReady) != 0;
+    h->fixed_dt = hd.next_dt;
     h->cfl_valid = (hd.flags & kFlagCflValid) != 0;
     if (p_out) *p_out = hd.params;
     return FVM_OK;

@@ -50,6 +50,10 @@ struct fvm_handle {
     // ping-pong buffers currently holds U^n)
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     unsigned long long graph_key[2] = {0, 0};
+    // graph replay of one step (single-step calls and odd remainders), per parity
+    cudaGraphExec_t graph1[2] = {nullptr, nullptr};
+    unsigned long long graph1_key[2] = {0, 0};
+    float fixed_dt = 0.0f;       // fixed policy: the dt sc->dt holds when dt_ready
     float *parity_base = nullptr;  // buffer holding U^n at parity 0
     // measurement
     bool timing = false;

@@ -349,6 +349,7 @@ def bench_serving(lams=(10.0, 100.0, 1000.0), n_req=24, chunk=64, budget=150 * 1
                               "completion_s_p50": q(solo_lat, 0.5), "completion_s_p99": q(solo_lat, 0.99),
                               "model": "FIFO single-solve queue on the same arrivals at measured per-class rates"},
             "speedup_vs_one_at_a_time": (work / span) / (solo_work / solo_span),
+            "batched_steps": st.batched_steps,
         })
     return {"sweep": sweep, "class_rates": {f"{k[0]}x{k[0] // 2}{'_ns' if k[1] else '_euler'}": v
                                             for k, v in class_rate.items()},
@@ -535,8 +536,11 @@ def run_many_solves(args, ws, rank, local, dist):
             "latency": {"completion_s_p50": top["completion_s_p50"], "completion_s_p99": top["completion_s_p99"],
                         "step_ms_p50": top["step_ms_p50"], "step_ms_p99": top["step_ms_p99"]},
             "sweep": r["sweep"], "class_rates": r["class_rates"],
-            "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": None,
-                    "d2h_bytes_per_step": None, "includes": "submit from host to final diagnostics on host"},
+            # per batched step: each request's parameters in (112 B), its result record out (184 B)
+            "e2e": {"value": value, "unit": "cell-updates/s",
+                    "h2d_bytes_per_step": args.requests * 112 / max(1, top["batched_steps"]),
+                    "d2h_bytes_per_step": args.requests * 184 / max(1, top["batched_steps"]),
+                    "includes": "submit from host to final diagnostics on host"},
         }
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -71,3 +71,10 @@ def test_create_without_device_reports_cuda_error():
 def test_build_info_names_the_target():
     lib = fvm_b200.load_library()
     assert b"sm_100a" in lib.fvm_build_info()
+
+
+def test_missing_library_fails_loudly(tmp_path, monkeypatch):
+    # no CPU fallback: without the built CUDA library the package refuses to run
+    monkeypatch.setattr(fvm_b200, "_lib", None)
+    with pytest.raises(fvm_b200.FvmError):
+        fvm_b200.load_library(str(tmp_path / "absent.so"))

@@ -1,0 +1,163 @@
+// fvm_pairx.cuh -- the two x-faces a stage-kernel thread evaluates per step
+// (same column, rows r and r+1) in packed FP32x2 arithmetic.
+//
+// sm_100 issues two FP32 adds, multiplies or FMAs per instruction
+// (__fadd2_rn / __fmul2_rn / __ffma2_rn) at the same FMA throughput as the
+// scalar forms, so packing saves issue slots, which is what the stage kernels
+// are bound by.  The primitive ring stores each row pair interleaved, {rho_r,
+// rho_r+1, u_r, u_r+1} and {v_r, v_r+1, p_r, p_r+1}, so one shared-memory
+// vector load yields both rows' operands as aligned register pairs and no
+// register moves are needed; lane .x is row r, lane .y row r+1.  Square
+// roots, reciprocals, min/max and the wave-fan selections stay per lane.
+//
+// The arithmetic is face_flux_sl + hllc_flux for an x-face (fvm_math.cuh;
+// reference computeFluxesKernel, src/solver.cu:1502-1598, and its HLLC,
+// :1112-1223) with explicit fused multiply-adds, so results can differ from
+// the scalar form in the last bits.
+#pragma once
+#include "fvm_math.cuh"
+
+namespace fvm {
+
+using f2 = float2;
+
+__device__ __forceinline__ f2 mk2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ f2 splat(float a) { return make_float2(a, a); }
+__device__ __forceinline__ f2 p_add(f2 a, f2 b) { return __fadd2_rn(a, b); }
+// a - b as a + b*(-1): one rounding, the value of a subtraction
+__device__ __forceinline__ f2 p_sub(f2 a, f2 b) { return __ffma2_rn(b, splat(-1.0f), a); }
+__device__ __forceinline__ f2 p_mul(f2 a, f2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ f2 p_fma(f2 a, f2 b, f2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ f2 p_min(f2 a, f2 b) { return mk2(fminf(a.x, b.x), fminf(a.y, b.y)); }
+__device__ __forceinline__ f2 p_max(f2 a, f2 b) { return mk2(fmaxf(a.x, b.x), fmaxf(a.y, b.y)); }
+__device__ __forceinline__ f2 p_max(f2 a, float b) { return mk2(fmaxf(a.x, b), fmaxf(a.y, b)); }
+__device__ __forceinline__ f2 p_sqrt(f2 a) { return mk2(sqrtf(a.x), sqrtf(a.y)); }
+// per-lane division a / b, the fast approximate form the scalar path uses
+__device__ __forceinline__ f2 p_div(f2 a, f2 b) { return mk2(__fdividef(a.x, b.x), __fdividef(a.y, b.y)); }
+__device__ __forceinline__ f2 p_sel(bool cx, bool cy, f2 a, f2 b) { return mk2(cx ? a.x : b.x, cy ? a.y : b.y); }
+
+// Limited slope per lane (as limited_slope).
+template <int LIM>
+__device__ __forceinline__ f2 p_slope(f2 qm1, f2 q0, f2 qp1) {
+    const f2 dL = p_sub(q0, qm1), dR = p_sub(qp1, q0);
+    if (LIM == 0) {
+        const f2 s = p_mul(splat(0.5f), p_add(mk2(copysignf(1.0f, dL.x), copysignf(1.0f, dL.y)),
+                                               mk2(copysignf(1.0f, dR.x), copysignf(1.0f, dR.y))));
+        return p_mul(s, mk2(fminf(fabsf(dL.x), fabsf(dR.x)), fminf(fabsf(dL.y), fabsf(dR.y))));
+    } else {
+        const f2 ab = p_mul(dL, dR);
+        const f2 q = p_div(p_mul(splat(2.0f), ab), p_add(dL, dR));
+        return mk2(ab.x > 0.0f ? q.x : 0.0f, ab.y > 0.0f ? q.y : 0.0f);
+    }
+}
+
+// Primitive states of one column for a row pair: lane .x row r, lane .y row r+1.
+struct PairPrim {
+    f2 rho, u, v, p;
+};
+__device__ __forceinline__ PairPrim pair_prim(const float4 &A, const float4 &B) {
+    return PairPrim{mk2(A.x, A.y), mk2(A.z, A.w), mk2(B.x, B.y), mk2(B.z, B.w)};
+}
+
+// x-faces of rows r (lane .x -> f0) and r+1 (lane .y -> f1) between cells
+// a | b, stencil m1, a, b, p2; out = {mass, x-momentum, y-momentum, energy,
+// rho_e}.  valid*: neither side a wall; near*: first order (wall at m1/p2).
+template <int SCHEME, int LIM>
+__device__ __forceinline__ void face_pair_x(bool valid0, bool near0, bool valid1, bool near1, const PairPrim &m1,
+                                            const PairPrim &a, const PairPrim &b, const PairPrim &p2, float f0[5],
+                                            float f1[5]) {
+    if (SCHEME != 0) {  // AUSM+: per lane through the scalar path
+        face_flux<true, SCHEME, LIM>(valid0, near0, Prim{m1.rho.x, m1.u.x, m1.v.x, m1.p.x},
+                                     Prim{a.rho.x, a.u.x, a.v.x, a.p.x}, Prim{b.rho.x, b.u.x, b.v.x, b.p.x},
+                                     Prim{p2.rho.x, p2.u.x, p2.v.x, p2.p.x}, f0);
+        face_flux<true, SCHEME, LIM>(valid1, near1, Prim{m1.rho.y, m1.u.y, m1.v.y, m1.p.y},
+                                     Prim{a.rho.y, a.u.y, a.v.y, a.p.y}, Prim{b.rho.y, b.u.y, b.v.y, b.p.y},
+                                     Prim{p2.rho.y, p2.u.y, p2.v.y, p2.p.y}, f1);
+        return;
+    }
+    const bool fo0 = near0 || a.rho.x < LOW_DENSITY || b.rho.x < LOW_DENSITY;
+    const bool fo1 = near1 || a.rho.y < LOW_DENSITY || b.rho.y < LOW_DENSITY;
+    const f2 hp = splat(0.5f);
+    const f2 omh = mk2(fo0 ? 0.0f : 0.5f, fo1 ? 0.0f : 0.5f);  // half order mask
+    // MUSCL: left = a + slope_a/2, right = b - slope_b/2
+    f2 rL = p_fma(p_slope<LIM>(m1.rho, a.rho, b.rho), omh, a.rho);
+    const f2 nL = p_fma(p_slope<LIM>(m1.u, a.u, b.u), omh, a.u);
+    const f2 tL = p_fma(p_slope<LIM>(m1.v, a.v, b.v), omh, a.v);
+    f2 pL = p_fma(p_slope<LIM>(m1.p, a.p, b.p), omh, a.p);
+    const f2 omm = mk2(-omh.x, -omh.y);
+    f2 rR = p_fma(p_slope<LIM>(a.rho, b.rho, p2.rho), omm, b.rho);
+    const f2 nR = p_fma(p_slope<LIM>(a.u, b.u, p2.u), omm, b.u);
+    const f2 tR = p_fma(p_slope<LIM>(a.v, b.v, p2.v), omm, b.v);
+    f2 pR = p_fma(p_slope<LIM>(a.p, b.p, p2.p), omm, b.p);
+    rL = p_max(rL, MIN_DENSITY);
+    pL = p_max(pL, MIN_PRESSURE);
+    rR = p_max(rR, MIN_DENSITY);
+    pR = p_max(pR, MIN_PRESSURE);
+    // E = p/(gamma-1) + rho*(u^2 + v^2)/2
+    const f2 igm1 = splat(1.0f / (GAMMA - 1.0f));
+    const f2 eL = p_mul(pL, igm1), eR = p_mul(pR, igm1);
+    const f2 EL = p_fma(p_mul(hp, rL), p_fma(nL, nL, p_mul(tL, tL)), eL);
+    const f2 ER = p_fma(p_mul(hp, rR), p_fma(nR, nR, p_mul(tR, tR)), eR);
+
+    // ---- HLLC with Roe-averaged Davis wave speeds
+    const f2 cL = p_sqrt(p_div(p_mul(splat(GAMMA), pL), rL));
+    const f2 cR = p_sqrt(p_div(p_mul(splat(GAMMA), pR), rR));
+    const f2 sqL = p_sqrt(rL), sqR = p_sqrt(rR);
+    const f2 den = p_add(p_add(sqL, sqR), splat(1e-10f));
+    const f2 un_roe = p_div(p_fma(sqL, nL, p_mul(sqR, nR)), den);
+    const f2 ut_roe = p_div(p_fma(sqL, tL, p_mul(sqR, tR)), den);
+    const f2 HL = p_div(p_add(EL, pL), rL), HR = p_div(p_add(ER, pR), rR);
+    const f2 H_roe = p_div(p_fma(sqL, HL, p_mul(sqR, HR)), den);
+    const f2 c2 = p_mul(splat(GAMMA - 1.0f), p_fma(splat(-0.5f), p_fma(un_roe, un_roe, p_mul(ut_roe, ut_roe)), H_roe));
+    const f2 c_avg = p_mul(hp, p_add(cL, cR));
+    const f2 c_roe = mk2(c2.x > 0.0f ? sqrtf(c2.x) : c_avg.x, c2.y > 0.0f ? sqrtf(c2.y) : c_avg.y);
+    f2 SL = p_min(p_sub(nL, cL), p_sub(un_roe, c_roe));
+    f2 SR = p_max(p_add(nR, cR), p_add(un_roe, c_roe));
+    const f2 delta = p_mul(splat(ENTROPY_FIX), p_max(cL, cR));
+    SL = mk2(fabsf(SL.x) < delta.x ? -delta.x : SL.x, fabsf(SL.y) < delta.y ? -delta.y : SL.y);
+    SR = mk2(fabsf(SR.x) < delta.x ? delta.x : SR.x, fabsf(SR.y) < delta.y ? delta.y : SR.y);
+    const f2 aL = p_sub(SL, nL), aR = p_sub(SR, nR);
+    const f2 mL = p_mul(rL, aL), mR = p_mul(rR, aR);
+    const f2 ds = p_sub(mL, mR);
+    const f2 sds = mk2(copysignf(fmaxf(fabsf(ds.x), 1e-10f), ds.x), copysignf(fmaxf(fabsf(ds.y), 1e-10f), ds.y));
+    const f2 Ss = p_div(p_sub(p_fma(mL, nL, p_sub(pR, pL)), p_mul(mR, nR)), sds);
+    // upwind side K of the wave fan (see hllc_flux)
+    const bool supL0 = SL.x >= 0.0f, supL1 = SL.y >= 0.0f;
+    const bool supR0 = !supL0 && SR.x <= 0.0f, supR1 = !supL1 && SR.y <= 0.0f;
+    const bool useL0 = supL0 || (!supR0 && Ss.x >= 0.0f), useL1 = supL1 || (!supR1 && Ss.y >= 0.0f);
+    const f2 rK = p_sel(useL0, useL1, rL, rR), nK = p_sel(useL0, useL1, nL, nR), tK = p_sel(useL0, useL1, tL, tR);
+    const f2 pK = p_sel(useL0, useL1, pL, pR), EK = p_sel(useL0, useL1, EL, ER), SK = p_sel(useL0, useL1, SL, SR);
+    const f2 d = p_sub(SK, nK);   // SK - unK
+    const f2 rkd = p_mul(rK, d);  // rK (SK - unK): the same product as mL / mR
+    const f2 fK0 = p_mul(rK, nK);
+    const f2 fK1 = p_fma(fK0, nK, pK);
+    const f2 fK2 = p_mul(fK0, tK);
+    const f2 fK3 = p_mul(p_add(EK, pK), nK);
+    f2 cd = p_sub(SK, Ss);
+    cd = mk2(fabsf(cd.x) < 1e-10f ? (cd.x >= 0.0f ? 1e-10f : -1e-10f) : cd.x,
+             fabsf(cd.y) < 1e-10f ? (cd.y >= 0.0f ? 1e-10f : -1e-10f) : cd.y);
+    const f2 rs = p_max(p_div(rkd, cd), MIN_DENSITY);
+    const f2 ps = p_max(p_fma(rkd, p_sub(Ss, nK), pK), MIN_PRESSURE);
+    const f2 Es = p_div(p_sub(p_fma(EK, d, p_mul(ps, Ss)), p_mul(pK, nK)), cd);
+    const bool st0 = !(supL0 || supR0), st1 = !(supL1 || supR1);
+    const f2 F0 = p_sel(st0, st1, p_fma(SK, p_sub(rs, rK), fK0), fK0);
+    const f2 Fn = p_sel(st0, st1, p_fma(SK, p_sub(p_mul(rs, Ss), fK0), fK1), fK1);
+    const f2 Ft = p_sel(st0, st1, p_fma(SK, p_mul(p_sub(rs, rK), tK), fK2), fK2);
+    const f2 F3 = p_sel(st0, st1, p_fma(SK, p_sub(Es, EK), fK3), fK3);
+    // upwinded internal-energy flux
+    const f2 uf = p_add(nL, nR);  // sign of 0.5 (unL + unR)
+    const f2 F4 = p_sel(uf.x >= 0.0f, uf.y >= 0.0f, p_mul(eL, nL), p_mul(eR, nR));
+    // wall faces: no mass/energy flux, x-momentum flux = pressure of the left cell
+    f0[0] = valid0 ? F0.x : 0.0f;
+    f0[1] = valid0 ? Fn.x : a.p.x;
+    f0[2] = valid0 ? Ft.x : 0.0f;
+    f0[3] = valid0 ? F3.x : 0.0f;
+    f0[4] = valid0 ? F4.x : 0.0f;
+    f1[0] = valid1 ? F0.y : 0.0f;
+    f1[1] = valid1 ? Fn.y : a.p.y;
+    f1[2] = valid1 ? Ft.y : 0.0f;
+    f1[3] = valid1 ? F3.y : 0.0f;
+    f1[4] = valid1 ? F4.y : 0.0f;
+}
+
+}  // namespace fvm

@@ -18,6 +18,7 @@
 #include <cstdio>
 
 #include "fvm_kernels.cuh"
+#include "fvm_pairx.cuh"
 #include "fvm_tma.cuh"
 
 namespace fvm {
@@ -150,7 +151,10 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
     static_assert(L::PP == 3 && L::XP == 1 && KP >= 2, "ring sizes");
     float *raw = reinterpret_cast<float *>(smem + L::raw_off);
     float *bl = reinterpret_cast<float *>(smem + L::bl_off);
-    float4 *P = reinterpret_cast<float4 *>(smem + L::p_off);
+    // primitives of a row pair, interleaved: PA = {rho_r, rho_r+1, u_r, u_r+1},
+    // PB = {v_r, v_r+1, p_r, p_r+1}, one float4 each per column and pair slot
+    float4 *PA = reinterpret_cast<float4 *>(smem + L::p_off);
+    float4 *PB = PA + L::PP * NT;
     float *X = reinterpret_cast<float *>(smem + L::x_off);
     uint8_t *M = smem + L::m_off;
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bar_off);
@@ -210,18 +214,21 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
         const uint32_t nA = __ldg(mcol + (size_t)clampi(r + 2, 0, ny - 1) * g.pitch);
         const uint32_t nB = __ldg(mcol + (size_t)clampi(r + 3, 0, ny - 1) * g.pitch);
         // ---- phase 1: primitives + masks of rows r, r+1
+        const int s0 = pc0 >> 1, s1 = pc1 >> 1, s2 = pc2 >> 1;  // pair slots of q, q-1, q-2
         bool ok = mbar_wait_bounded(&bars[kr], (uint32_t)par);
         if (ok) {
+            float rho[2], u[2], v[2], p[2];
 #pragma unroll
             for (int h = 0; h < 2; h++) {
                 const float *src = raw + (size_t)(kr * 2 + h) * L::SLOT;
-                float u, v, p, T;
-                const float rho = ring_at<L::NB>(src, 0, rc_t);
-                prim_from_cons(rho, ring_at<L::NB>(src, 1, rc_t), ring_at<L::NB>(src, 2, rc_t),
-                               ring_at<L::NB>(src, 3, rc_t), ring_at<L::NB>(src, 4, rc_t), u, v, p, T);
-                P[(pc0 + h) * NT + t] = make_float4(rho, u, v, p);
+                float T;
+                rho[h] = ring_at<L::NB>(src, 0, rc_t);
+                prim_from_cons(rho[h], ring_at<L::NB>(src, 1, rc_t), ring_at<L::NB>(src, 2, rc_t),
+                               ring_at<L::NB>(src, 3, rc_t), ring_at<L::NB>(src, 4, rc_t), u[h], v[h], p[h], T);
                 M[(pc0 + h) * NT + t] = (uint8_t)(h ? mB : mA);
             }
+            PA[s0 * NT + t] = make_float4(rho[0], rho[1], u[0], u[1]);
+            PB[s0 * NT + t] = make_float4(v[0], v[1], p[0], p[1]);
         }
         mA = nA;
         mB = nB;
@@ -230,13 +237,22 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
             break;
         }
         // ---- phase 2: y-faces of column cy, then the update of rows r-2, r-1
-        const float4 c3 = P[(pc2 + 1) * NT + cy];  // column cy, row r-3
-        const float4 c2 = P[pc1 * NT + cy];        // r-2
-        const float4 c1 = P[(pc1 + 1) * NT + cy];  // r-1
-        const float4 c0 = P[pc0 * NT + cy];        // r
+        float4 c3, c2, c1, c0, cp;  // column cy, rows r-3 .. r+1 as (rho, u, v, p)
+        {
+            const float4 A2 = PA[s2 * NT + cy], B2 = PB[s2 * NT + cy];
+            const float4 A1 = PA[s1 * NT + cy], B1 = PB[s1 * NT + cy];
+            const float4 A0 = PA[s0 * NT + cy], B0 = PB[s0 * NT + cy];
+            c3 = make_float4(A2.y, A2.w, B2.y, B2.w);
+            c2 = make_float4(A1.x, A1.z, B1.x, B1.z);
+            c1 = make_float4(A1.y, A1.w, B1.y, B1.w);
+            c0 = make_float4(A0.x, A0.z, B0.x, B0.z);
+            cp = make_float4(A0.y, A0.w, B0.y, B0.w);
+        }
+        // densities of rows r-2, r-1 beside column cy
+        const float2 rhoE = *reinterpret_cast<const float2 *>(&PA[s1 * NT + cy + 1]);
+        const float2 rhoW = *reinterpret_cast<const float2 *>(&PA[s1 * NT + cy - 1]);
         float fy0[5], fy1[5];
         {
-            const float4 cp = P[(pc0 + 1) * NT + cy];  // r+1
             const uint32_t my0 = M[pc1 * NT + cy], my1 = M[(pc1 + 1) * NT + cy];
             // y-slopes of rows r-1 and r; those of row r-2 are row r of step q-1
             const Prim q2{c2.x, c2.y, c2.z, c2.w}, q1{c1.x, c1.y, c1.z, c1.w}, q0{c0.x, c0.y, c0.z, c0.w};
@@ -271,7 +287,7 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
                         fB[k] = h ? fy0[k] : fyB[k];
                     }
                     const float4 pc = h ? c1 : c2;
-                    const float rxR = P[(pc1 + h) * NT + cy + 1].x, rxL = P[(pc1 + h) * NT + cy - 1].x;
+                    const float rxR = h ? rhoE.y : rhoE.x, rxL = h ? rhoW.y : rhoW.x;
                     const float ryT = h ? c0.x : c1.x;
                     const float ryB = h ? c2.x : c3.x;
                     const bool edge_y = (urow == 0 || urow == ny - 1);
@@ -307,15 +323,11 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
         // ---- phase 3: x-faces of rows r, r+1 (read by the update in step q+1)
         {
             float fx0[5], fx1[5];
-#pragma unroll
-            for (int h = 0; h < 2; h++) {
-                const float4 *Pr = P + (pc0 + h) * NT;
-                const uint32_t mbx = M[(pc0 + h) * NT + tx + 1];
-                const float4 xm1 = Pr[tx], xa = Pr[tx + 1], xb = Pr[tx + 2], xp2 = Pr[tx + 3];
-                face_flux<true, SCHEME, LIM>((mbx & MB_XV) != 0, (mbx & MB_XN) != 0, Prim{xm1.x, xm1.y, xm1.z, xm1.w},
-                                             Prim{xa.x, xa.y, xa.z, xa.w}, Prim{xb.x, xb.y, xb.z, xb.w},
-                                             Prim{xp2.x, xp2.y, xp2.z, xp2.w}, h ? fx1 : fx0);
-            }
+            const float4 *A = PA + s0 * NT, *B = PB + s0 * NT;
+            const uint32_t mb0 = M[pc0 * NT + tx + 1], mb1 = M[(pc0 + 1) * NT + tx + 1];
+            face_pair_x<SCHEME, LIM>((mb0 & MB_XV) != 0, (mb0 & MB_XN) != 0, (mb1 & MB_XV) != 0, (mb1 & MB_XN) != 0,
+                                     pair_prim(A[tx], B[tx]), pair_prim(A[tx + 1], B[tx + 1]),
+                                     pair_prim(A[tx + 2], B[tx + 2]), pair_prim(A[tx + 3], B[tx + 3]), fx0, fx1);
             if (t <= W) {
                 float *Xs = X + t;
 #pragma unroll
@@ -346,7 +358,7 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
 }
 
 template <int NT, int K, int STAGE, int SCHEME, int LIM>
-__global__ void __launch_bounds__(NT) k_stage(const __grid_constant__ CUtensorMap tm_in,
+__global__ void __launch_bounds__(NT, 640 / NT) k_stage(const __grid_constant__ CUtensorMap tm_in,
                                               const __grid_constant__ CUtensorMap tm_blend, const StepArgs a) {
     using L = StageLayout<NT, K, STAGE>;
     static_assert(L::total <= 227 * 1024, "shared memory");

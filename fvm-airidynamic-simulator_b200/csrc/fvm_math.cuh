@@ -551,11 +551,11 @@ struct ViscArgs {
     float inv_2dx, inv_2dy, inv_dx, inv_dy, prandtl;
     bool ref_prandtl;
 };
-__device__ __forceinline__ void stress_heat(float uC, float vC, float TC, float uE, float uW, float uN, float uS,
-                                            float vE, float vW, float vN, float vS, float TE, float TW, float TN,
-                                            float TS, bool i_lo, bool i_hi, bool j_lo, bool j_hi,
-                                            const ViscArgs &va, float out[5]) {
-    float mu_val = sutherland_mu(TC);
+// `mu_val` is sutherland_mu(TC), computed by the caller.
+__device__ __forceinline__ void stress_heat_mu(float mu_val, float uC, float vC, float TC, float uE, float uW,
+                                               float uN, float uS, float vE, float vW, float vN, float vS, float TE,
+                                               float TW, float TN, float TS, bool i_lo, bool i_hi, bool j_lo,
+                                               bool j_hi, const ViscArgs &va, float out[5]) {
     float k_val = va.ref_prandtl ? (mu_val * CP / PRANDTL_REF) : (mu_val * CP / va.prandtl);
     float du_dx = (uE - uW) * va.inv_2dx;
     float du_dy = (uN - uS) * va.inv_2dy;
@@ -591,6 +591,13 @@ __device__ __forceinline__ void stress_heat(float uC, float vC, float TC, float 
         dT_dy = (TC - TS) * va.inv_dy;
     out[3] = -k_val * dT_dx;
     out[4] = -k_val * dT_dy;
+}
+__device__ __forceinline__ void stress_heat(float uC, float vC, float TC, float uE, float uW, float uN, float uS,
+                                            float vE, float vW, float vN, float vS, float TE, float TW, float TN,
+                                            float TS, bool i_lo, bool i_hi, bool j_lo, bool j_hi,
+                                            const ViscArgs &va, float out[5]) {
+    stress_heat_mu(sutherland_mu(TC), uC, vC, TC, uE, uW, uN, uS, vE, vW, vN, vS, TE, TW, TN, TS, i_lo, i_hi, j_lo,
+                   j_hi, va, out);
 }
 
 // Divergence + forward Euler of the viscous half step for an interior fluid

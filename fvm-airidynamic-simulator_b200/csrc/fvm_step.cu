@@ -404,23 +404,26 @@ struct ViscLayout {
 
 // Viscous half step on one tile (fusedViscousDiffusionKernel,
 // src/solver.cu:2251-2511), out of place, marching two rows per step.
-// Per step q (incoming rows r = j0-2+2q and r+1):
-//   phase 1  primitives (u, v, T) + masks of rows r, r+1 on NT columns; the
-//            thread also keeps the conserved state of rows r, r+1 at the
-//            column it updates one step later, so the input slot is free
-//            after the first barrier and is refilled there
+// Thread t owns column i0-2+t in every phase.  Per step q (incoming rows
+// r = j0-2+2q and r+1):
+//   phase 1  primitives (u, v, T) and Sutherland viscosity + masks of rows
+//            r, r+1 on NT columns; the thread keeps the conserved state of
+//            rows r, r+1 of its column for its update one step later, so the
+//            input slot is free after the first barrier and is refilled there
 //   -- barrier --
 //   phase 2  stress and heat flux of rows r-1, r on NT-2 columns
 //   -- barrier --
-//   phase 3  viscous update of rows r-2, r-1 on W columns
+//   phase 3  viscous update of rows r-2, r-1 on the W = NT-4 middle columns
+// Both rows of a phase are evaluated in straight-line code (validity applied
+// by selects and predicated stores), so their dependency chains interleave.
 template <int NT, int K>
 __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const StepArgs &a, int i0, int j0,
                                              unsigned char *smem, RingPos &rp, float &lmax_speed, float &lmax_nu) {
     using L = ViscLayout<NT, K>;
-    constexpr int W = L::W, KP = L::KP;
+    constexpr int KP = L::KP;
     static_assert(L::PP == 3 && L::TP == 2 && KP >= 2, "ring sizes");
     float *raw = reinterpret_cast<float *>(smem + L::raw_off);
-    float4 *P = reinterpret_cast<float4 *>(smem + L::p_off);  // {u, v, T, -}
+    float4 *P = reinterpret_cast<float4 *>(smem + L::p_off);  // {u, v, T, mu}
     float *Tq = reinterpret_cast<float *>(smem + L::t_off);   // {txx, tyy, txy, qx, qy}
     uint8_t *M = smem + L::m_off;
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bar_off);
@@ -460,23 +463,23 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
     if (t == 0)
         for (int q = 0; q < issued; q++) issue(q);
 
-    const int ic_t = clampi(i0 - 2 + t, 0, nx - 1);
-    const int rc_t = ic_t - i0 + 4;
+    const int ic = i0 - 2 + t;                  // this thread's column
+    const int ic_t = clampi(ic, 0, nx - 1);     // column whose state it loads
+    const int rc_t = ic_t - i0 + 4;             // its staged position
     const uint8_t *mcol = a.mask + ic_t;
     uint32_t mA = __ldg(mcol + (size_t)clampi(rs, 0, ny - 1) * g.pitch);
     uint32_t mB = __ldg(mcol + (size_t)clampi(rs + 1, 0, ny - 1) * g.pitch);
-    const int is = i0 - 1 + t;
-    const bool stress_col_in = (t < NT - 2) && is >= 0 && is < nx;
-    const int iu = i0 + t;
-    const bool col_ok = (t < W) && (iu < nx);
-    const bool interior_x = iu > 0 && iu < nx - 1;
-    const int uc = min(t, W - 1) + 4;  // staged column of the updated cell
-    float *outp = a.out + iu;
+    const bool stress_thread = t >= 1 && t < NT - 1;
+    const bool stress_col_in = ic >= 0 && ic < nx;
+    const bool i_lo = ic == 0, i_hi = ic == nx - 1;
+    const bool col_ok = t >= 2 && t < NT - 2 && ic < nx;
+    const bool interior_x = ic > 0 && ic < nx - 1;
+    const int tp = min(max(t, 1), NT - 2);  // stencil centre kept inside the rings
 
     int kr = base % KP, par = (base / KP) & 1;
     int pc0 = 0, pc1 = 4, pc2 = 2;  // P/M rows of row pairs q, q-1, q-2
     int tc0 = 0, tc1 = 2;           // stress rows of row pairs q (rows r-1, r) and q-1
-    float Uprev[2][5];              // conserved state of rows r-2, r-1 at column iu
+    float Uprev[2][5];              // conserved state of rows r-2, r-1 at column ic
 #pragma unroll
     for (int h = 0; h < 2; h++)
 #pragma unroll
@@ -487,21 +490,19 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
         const int r = rs + 2 * q;
         const uint32_t nA = __ldg(mcol + (size_t)clampi(r + 2, 0, ny - 1) * g.pitch);
         const uint32_t nB = __ldg(mcol + (size_t)clampi(r + 3, 0, ny - 1) * g.pitch);
-        // ---- phase 1: primitives + masks of rows r, r+1; conserved state for step q+1
+        // ---- phase 1: primitives, viscosity and masks of rows r, r+1
         float Unext[2][5];
         bool ok = mbar_wait_bounded(&bars[kr], (uint32_t)par);
         if (ok) {
 #pragma unroll
             for (int h = 0; h < 2; h++) {
                 const float *src = raw + (size_t)(kr * 2 + h) * L::SLOT;
-                float u, v, p, T;
-                prim_from_cons(ring_at<L::NB>(src, 0, rc_t), ring_at<L::NB>(src, 1, rc_t),
-                               ring_at<L::NB>(src, 2, rc_t), ring_at<L::NB>(src, 3, rc_t),
-                               ring_at<L::NB>(src, 4, rc_t), u, v, p, T);
-                P[(pc0 + h) * NT + t] = make_float4(u, v, T, 0.0f);
-                M[(pc0 + h) * NT + t] = (uint8_t)(h ? mB : mA);
 #pragma unroll
-                for (int k = 0; k < 5; k++) Unext[h][k] = ring_at<L::NB>(src, k, uc);
+                for (int k = 0; k < 5; k++) Unext[h][k] = ring_at<L::NB>(src, k, rc_t);
+                float u, v, p, T;
+                prim_from_cons(Unext[h][0], Unext[h][1], Unext[h][2], Unext[h][3], Unext[h][4], u, v, p, T);
+                P[(pc0 + h) * NT + t] = make_float4(u, v, T, sutherland_mu(T));
+                M[(pc0 + h) * NT + t] = (uint8_t)(h ? mB : mA);
             }
         } else {
 #pragma unroll
@@ -521,87 +522,96 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
             issue(issued);
             ++issued;
         }
-        // ---- phase 2: stress and heat flux of rows r-1, r at column i0-1+t
-        if (t < NT - 2) {
-            const int c = t + 1;
+        // ---- phase 2: stress and heat flux of rows r-1, r at column ic
+        // (step 0 holds rows j0-3, j0-2, which no update of this tile reads)
+        if (stress_thread && q > 0) {
+            float out[2][5];
 #pragma unroll
             for (int h = 0; h < 2; h++) {
                 const int trow = r - 1 + h;
-                if (trow >= j0 - 1) {
-                    // rows trow-1, trow, trow+1 of the primitive ring
-                    const int rowS = h ? pc1 + 1 : pc1, rowC = h ? pc0 : pc1 + 1, rowN = h ? pc0 + 1 : pc0;
-                    float out[5];
-                    const uint32_t ct = mb_type(M[rowC * NT + c]);
-                    if (!stress_col_in || trow < 0 || trow >= ny || ct == CT_SOLID) {
+                // rows trow-1, trow, trow+1 of the primitive ring
+                const int rowS = h ? pc1 + 1 : pc1, rowC = h ? pc0 : pc1 + 1, rowN = h ? pc0 + 1 : pc0;
+                const float4 C = P[rowC * NT + t], E = P[rowC * NT + t + 1], Wc = P[rowC * NT + t - 1];
+                const float4 N = P[rowN * NT + t], S = P[rowS * NT + t];
+                stress_heat_mu(C.w, C.x, C.y, C.z, E.x, Wc.x, N.x, S.x, E.y, Wc.y, N.y, S.y, E.z, Wc.z, N.z, S.z,
+                               i_lo, i_hi, trow == 0, trow == ny - 1, va, out[h]);
+                const bool live = stress_col_in && trow >= 0 && trow < ny &&
+                                  mb_type(M[rowC * NT + t]) != CT_SOLID;
 #pragma unroll
-                        for (int k = 0; k < 5; k++) out[k] = 0.0f;
-                    } else {
-                        const float4 C = P[rowC * NT + c], E = P[rowC * NT + c + 1], Wc = P[rowC * NT + c - 1];
-                        const float4 N = P[rowN * NT + c], S = P[rowS * NT + c];
-                        stress_heat(C.x, C.y, C.z, E.x, Wc.x, N.x, S.x, E.y, Wc.y, N.y, S.y, E.z, Wc.z, N.z, S.z,
-                                    is == 0, is == nx - 1, trow == 0, trow == ny - 1, va, out);
-                    }
-                    float *Ts = Tq + (tc0 + h) * 5 * NT + t;
+                for (int k = 0; k < 5; k++) out[h][k] = live ? out[h][k] : 0.0f;
+            }
 #pragma unroll
-                    for (int k = 0; k < 5; k++) Ts[k * NT] = out[k];
-                }
+            for (int h = 0; h < 2; h++) {
+                float *Ts = Tq + (tc0 + h) * 5 * NT + t;
+#pragma unroll
+                for (int k = 0; k < 5; k++) Ts[k * NT] = out[h][k];
             }
         }
         // south neighbour of row r-2 (row r-3, pair q-2): read before its slot is reused
-        const float4 S0 = P[(pc2 + 1) * NT + min(t, W - 1) + 2];
+        const float4 S0 = P[(pc2 + 1) * NT + tp];
         __syncthreads();
-        // ---- phase 3: viscous update of rows r-2, r-1 at column i0+t
+        // ---- phase 3: viscous update of rows r-2, r-1 at column ic (rows
+        // of this tile from step 2 on)
+        if (q >= 2) {
+            float U[2][5];
+            uint32_t ctype[2];
+            bool store[2];
 #pragma unroll
-        for (int h = 0; h < 2; h++) {
-            const int urow = r - 2 + h;
-            if (urow >= j0 && urow < j1 && col_ok) {
-                const int c = t + 2;   // primitive column
-                const int tc = t + 1;  // stress column
+            for (int h = 0; h < 2; h++) {
+                const int urow = r - 2 + h;
                 const int prow = pc1 + h;
-                const uint32_t mb = M[prow * NT + c];
-                const uint32_t ctype = mb_type(mb);
-                float U[5];
+                store[h] = col_ok && urow >= j0 && urow < j1;
+                ctype[h] = mb_type(M[prow * NT + tp]);
+                // stress rows urow-1, urow, urow+1
+                const int tS = h ? tc1 + 1 : tc1, tC0 = h ? tc0 : tc1 + 1, tN = h ? tc0 + 1 : tc0;
+                const float *T0 = Tq + tC0 * 5 * NT + tp;
+                const float *TN = Tq + tN * 5 * NT + tp;
+                const float *TS = Tq + tS * 5 * NT + tp;
+                float tC[5], tE[5], tW[5], tNn[5], tSs[5];
 #pragma unroll
-                for (int k = 0; k < 5; k++) U[k] = Uprev[h][k];
-                const float4 pc = P[prow * NT + c];
-                if (ctype == CT_FLUID && interior_x && urow > 0 && urow < ny - 1) {
-                    // stress rows urow-1, urow, urow+1
-                    const int tS = h ? tc1 + 1 : tc1, tC0 = h ? tc0 : tc1 + 1, tN = h ? tc0 + 1 : tc0;
-                    const float *T0 = Tq + tC0 * 5 * NT + tc;
-                    const float *TN = Tq + tN * 5 * NT + tc;
-                    const float *TS = Tq + tS * 5 * NT + tc;
-                    float tC[5], tE[5], tW[5], tNn[5], tSs[5];
-#pragma unroll
-                    for (int k = 0; k < 5; k++) {
-                        tC[k] = T0[k * NT];
-                        tE[k] = T0[k * NT + 1];
-                        tW[k] = T0[k * NT - 1];
-                        tNn[k] = TN[k * NT];
-                        tSs[k] = TS[k * NT];
-                    }
-                    const float4 E = P[prow * NT + c + 1], Wc = P[prow * NT + c - 1];
-                    const float4 N = P[(h ? pc0 : pc1 + 1) * NT + c];
-                    const float4 S = h ? P[pc1 * NT + c] : S0;
-                    float rhs[4];
-                    viscous_rhs(tC, tE, tW, tNn, tSs, E.x, Wc.x, N.x, S.x, E.y, Wc.y, N.y, S.y, va, rhs);
-                    U[1] += dt * rhs[0];
-                    U[2] += dt * rhs[1];
-                    U[3] += dt * rhs[2];
-                    U[4] += dt * rhs[3];
+                for (int k = 0; k < 5; k++) {
+                    tC[k] = T0[k * NT];
+                    tE[k] = T0[k * NT + 1];
+                    tW[k] = T0[k * NT - 1];
+                    tNn[k] = TN[k * NT];
+                    tSs[k] = TS[k * NT];
                 }
-                if (a.apply_bc) bc_pointwise(U, ctype, iu, urow, nx, ny, a.fs);
-                if (a.cfl && ctype != CT_GHOST) {
+                const float4 E = P[prow * NT + tp + 1], Wc = P[prow * NT + tp - 1];
+                const float4 N = P[(h ? pc0 : pc1 + 1) * NT + tp];
+                const float4 S = h ? P[pc1 * NT + tp] : S0;
+                float rhs[4];
+                viscous_rhs(tC, tE, tW, tNn, tSs, E.x, Wc.x, N.x, S.x, E.y, Wc.y, N.y, S.y, va, rhs);
+                const bool upd = ctype[h] == CT_FLUID && interior_x && urow > 0 && urow < ny - 1;
+                U[h][0] = Uprev[h][0];
+#pragma unroll
+                for (int k = 1; k < 5; k++) U[h][k] = upd ? Uprev[h][k] + dt * rhs[k - 1] : Uprev[h][k];
+            }
+            if (a.apply_bc) {
+#pragma unroll
+                for (int h = 0; h < 2; h++) bc_pointwise(U[h], ctype[h], ic, r - 2 + h, nx, ny, a.fs);
+            }
+            if (a.cfl) {
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
                     float uu, vv, pp, TT;
-                    prim_from_cons(U[0], U[1], U[2], U[3], U[4], uu, vv, pp, TT);
-                    lmax_speed = fmaxf(lmax_speed, wave_speed(uu, vv, pp, U[0]));
+                    prim_from_cons(U[h][0], U[h][1], U[h][2], U[h][3], U[h][4], uu, vv, pp, TT);
+                    const bool counted = store[h] && ctype[h] != CT_GHOST;
+                    const float ws = wave_speed(uu, vv, pp, U[h][0]);
+                    lmax_speed = counted ? fmaxf(lmax_speed, ws) : lmax_speed;
                     if (a.cfl == 2) {
-                        const float mu = (ctype == CT_SOLID) ? 0.0f : sutherland_mu(pc.z);
-                        lmax_nu = fmaxf(lmax_nu, mu / (U[0] + 1e-10f));
+                        const float mu = (ctype[h] == CT_SOLID) ? 0.0f : P[(pc1 + h) * NT + tp].w;
+                        const float nu = mu / (U[h][0] + 1e-10f);
+                        lmax_nu = counted ? fmaxf(lmax_nu, nu) : lmax_nu;
                     }
                 }
-                float *dst = outp + (size_t)urow * g.pitch;
+            }
 #pragma unroll
-                for (int k = 0; k < 5; k++) dst[k * g.plane] = U[k];
+            for (int h = 0; h < 2; h++) {
+                if (store[h]) {
+                    float *dst = a.out + (size_t)(r - 2 + h) * g.pitch + ic;
+#pragma unroll
+                    for (int k = 0; k < 5; k++) dst[k * g.plane] = U[h][k];
+                }
             }
         }
 #pragma unroll

@@ -592,6 +592,26 @@ __device__ __forceinline__ void stress_heat_mu(float mu_val, float uC, float vC,
     out[3] = -k_val * dT_dx;
     out[4] = -k_val * dT_dy;
 }
+// The same stress and heat flux with the edge choice made by the caller: at a
+// left (bottom) domain edge the west (south) neighbour passed is the cell
+// itself and fx (fy) = 1/dx (1/dy); at a right (top) edge the east (north)
+// one, likewise; in the interior the neighbours and 1/(2dx), 1/(2dy).  Every
+// difference is then the one stress_heat_mu takes, with identical operations.
+__device__ __forceinline__ void stress_heat_sel(float mu_val, float uE, float uW, float uN, float uS, float vE,
+                                                float vW, float vN, float vS, float TE, float TW, float TN, float TS,
+                                                float fx, float fy, const ViscArgs &va, float out[5]) {
+    float k_val = va.ref_prandtl ? (mu_val * CP / PRANDTL_REF) : (mu_val * CP / va.prandtl);
+    float du_dx = (uE - uW) * fx;
+    float du_dy = (uN - uS) * fy;
+    float dv_dx = (vE - vW) * fx;
+    float dv_dy = (vN - vS) * fy;
+    float div_v = du_dx + dv_dy;
+    out[0] = mu_val * (2.0f * du_dx - (2.0f / 3.0f) * div_v);
+    out[1] = mu_val * (2.0f * dv_dy - (2.0f / 3.0f) * div_v);
+    out[2] = mu_val * (du_dy + dv_dx);
+    out[3] = -k_val * ((TE - TW) * fx);
+    out[4] = -k_val * ((TN - TS) * fy);
+}
 __device__ __forceinline__ void stress_heat(float uC, float vC, float TC, float uE, float uW, float uN, float uS,
                                             float vE, float vW, float vN, float vS, float TE, float TW, float TN,
                                             float TS, bool i_lo, bool i_hi, bool j_lo, bool j_hi,

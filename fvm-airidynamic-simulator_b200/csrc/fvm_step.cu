@@ -357,9 +357,12 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
     return true;
 }
 
+// Occupancy targets: 6 CTAs of 128 threads per SM for stage 1 (80 registers,
+// no spills), 5 for stage 2, whose blend ring leaves shared memory for 5.
 template <int NT, int K, int STAGE, int SCHEME, int LIM>
-__global__ void __launch_bounds__(NT, 640 / NT) k_stage(const __grid_constant__ CUtensorMap tm_in,
-                                              const __grid_constant__ CUtensorMap tm_blend, const StepArgs a) {
+__global__ void __launch_bounds__(NT, (STAGE == 1 ? 768 : 640) / NT)
+    k_stage(const __grid_constant__ CUtensorMap tm_in, const __grid_constant__ CUtensorMap tm_blend,
+            const StepArgs a) {
     using L = StageLayout<NT, K, STAGE>;
     static_assert(L::total <= 227 * 1024, "shared memory");
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -472,6 +475,10 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
     const bool stress_thread = t >= 1 && t < NT - 1;
     const bool stress_col_in = ic >= 0 && ic < nx;
     const bool i_lo = ic == 0, i_hi = ic == nx - 1;
+    // x-differences of the stress: one-sided at the domain edges (the cell
+    // itself stands in for the missing neighbour), central elsewhere
+    const int tW = i_lo ? t : t - 1, tE = (i_hi && !i_lo) ? t : t + 1;
+    const float fx = (i_lo || i_hi) ? va.inv_dx : va.inv_2dx;
     const bool col_ok = t >= 2 && t < NT - 2 && ic < nx;
     const bool interior_x = ic > 0 && ic < nx - 1;
     const int tp = min(max(t, 1), NT - 2);  // stencil centre kept inside the rings
@@ -529,12 +536,18 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
 #pragma unroll
             for (int h = 0; h < 2; h++) {
                 const int trow = r - 1 + h;
-                // rows trow-1, trow, trow+1 of the primitive ring
-                const int rowS = h ? pc1 + 1 : pc1, rowC = h ? pc0 : pc1 + 1, rowN = h ? pc0 + 1 : pc0;
-                const float4 C = P[rowC * NT + t], E = P[rowC * NT + t + 1], Wc = P[rowC * NT + t - 1];
+                // rows trow-1, trow, trow+1 of the primitive ring; at the
+                // bottom (top) domain edge the row itself replaces the south
+                // (north) one and the y-difference is one-sided
+                const bool j_lo = trow == 0, j_hi = trow == ny - 1 && !j_lo;
+                const int rowC = h ? pc0 : pc1 + 1;
+                const int rowS = j_lo ? rowC : (h ? pc1 + 1 : pc1);
+                const int rowN = j_hi ? rowC : (h ? pc0 + 1 : pc0);
+                const float fy = (j_lo || j_hi) ? va.inv_dy : va.inv_2dy;
+                const float4 C = P[rowC * NT + t], E = P[rowC * NT + tE], Wc = P[rowC * NT + tW];
                 const float4 N = P[rowN * NT + t], S = P[rowS * NT + t];
-                stress_heat_mu(C.w, C.x, C.y, C.z, E.x, Wc.x, N.x, S.x, E.y, Wc.y, N.y, S.y, E.z, Wc.z, N.z, S.z,
-                               i_lo, i_hi, trow == 0, trow == ny - 1, va, out[h]);
+                stress_heat_sel(C.w, E.x, Wc.x, N.x, S.x, E.y, Wc.y, N.y, S.y, E.z, Wc.z, N.z, S.z, fx, fy, va,
+                                out[h]);
                 const bool live = stress_col_in && trow >= 0 && trow < ny &&
                                   mb_type(M[rowC * NT + t]) != CT_SOLID;
 #pragma unroll
@@ -688,10 +701,11 @@ __device__ __forceinline__ StepArgs batch_args(const BatchInst &I, int out_role,
 }
 
 template <int NT, int K, int STAGE, int SCHEME, int LIM>
-__global__ void __launch_bounds__(NT) k_stage_batch(const BatchInst *__restrict__ insts,
+__global__ void __launch_bounds__(NT, 640 / NT) k_stage_batch(const BatchInst *__restrict__ insts,
                                                     const TileDesc *__restrict__ tiles, int ntiles, int rows) {
     using L = StageLayout<NT, K, STAGE>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ StepArgs s_args;
     unsigned char *smem = aligned_smem(smem_raw);
     if (smem_misaligned(smem, insts[0].sc)) return;
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bar_off);
@@ -718,21 +732,25 @@ __global__ void __launch_bounds__(NT) k_stage_batch(const BatchInst *__restrict_
             bc = visc ? 0 : 1;
             cfl = visc ? 0 : 1;
         }
-        const StepArgs a = batch_args(I, out_role, bc, cfl, 1.0f, rows);
+        // the tile's arguments live in shared memory, not in registers
+        __syncthreads();  // every thread is done with the previous tile's arguments
+        if (threadIdx.x == 0) s_args = batch_args(I, out_role, bc, cfl, 1.0f, rows);
+        __syncthreads();
         float lmax = 0.0f;
         if (!stage_tile<NT, K, STAGE, SCHEME, LIM>(&I.tm_in[role_buf(I, in_role)], &I.tm_ctr[role_buf(I, blend_role)],
-                                                   a, td.i0, td.j0, smem, rp, lmax))
+                                                   s_args, td.i0, td.j0, smem, rp, lmax))
             return;
         if (cfl) block_max2_publish<NT>(lmax, 0.0f, I.sc->red);
     }
 }
 
 template <int NT, int K>
-__global__ void __launch_bounds__(NT) k_viscous_batch(const BatchInst *__restrict__ insts,
+__global__ void __launch_bounds__(NT, 640 / NT) k_viscous_batch(const BatchInst *__restrict__ insts,
                                                       const TileDesc *__restrict__ tiles, int ntiles, int rows,
                                                       int post) {
     using L = ViscLayout<NT, K>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ StepArgs s_args;
     unsigned char *smem = aligned_smem(smem_raw);
     if (smem_misaligned(smem, insts[0].sc)) return;
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bar_off);
@@ -746,9 +764,11 @@ __global__ void __launch_bounds__(NT) k_viscous_batch(const BatchInst *__restric
         const BatchInst &I = insts[td.inst];
         // pre: U^n -> U_d (no BC); post: U_b -> U^{n+1} with BC and CFL
         const int in_role = post ? ROLE_D : ROLE_N;
-        const StepArgs a = batch_args(I, post ? ROLE_X : ROLE_D, post, post ? 2 : 0, 0.5f, rows);
+        __syncthreads();  // every thread is done with the previous tile's arguments
+        if (threadIdx.x == 0) s_args = batch_args(I, post ? ROLE_X : ROLE_D, post, post ? 2 : 0, 0.5f, rows);
+        __syncthreads();
         float ls = 0.0f, ln = 0.0f;
-        if (!viscous_tile<NT, K>(&I.tm_in[role_buf(I, in_role)], a, td.i0, td.j0, smem, rp, ls, ln)) return;
+        if (!viscous_tile<NT, K>(&I.tm_in[role_buf(I, in_role)], s_args, td.i0, td.j0, smem, rp, ls, ln)) return;
         if (post) block_max2_publish<NT>(ls, ln, I.sc->red);
     }
 }

@@ -262,7 +262,8 @@ static StageTune pick_tune(const fvm_handle *h, int nx, int ny) {
     const char *env = getenv("FVM_TUNE");
     if (env) {
         int x = 0, y = 0, z = 0;
-        if (sscanf(env, "%d,%d,%d", &x, &y, &z) == 3 && (x == 128 || x == 256) && (y == 4 || y == 6) && z >= 4)
+        if (sscanf(env, "%d,%d,%d", &x, &y, &z) == 3 && (x == 128 || x == 256) && (y == 4 || y == 6) && z >= 4 &&
+            (z & 1) == 0)
             return StageTune{x, y, z};
     }
     TuneKey k{nx, ny, h->prm.enable_viscosity ? 1 : 0, h->ext.flux_scheme, h->ext.limiter};
@@ -1071,6 +1072,17 @@ extern "C" int fvm_autotune(fvm_handle *h, const fvm_sim_params *p, int steps, f
         best;
     if (best_ms_out) *best_ms_out = best_ms;
     return FVM_OK;
+}
+
+extern "C" int fvm_set_tune(fvm_handle *h, int nt, int ring, int rows) {
+    CHECK_INIT(h);
+    if (!(nt == 128 || nt == 256) || !(ring == 4 || ring == 6) || rows < 4 || rows > 65536 || (rows & 1))
+        return set_err(FVM_ERR_INVALID,
+                       "fvm_set_tune: threads 128 or 256, ring 4 or 6, even rows 4..65536 (got %d, %d, %d)", nt, ring,
+                       rows);
+    h->tune = StageTune{nt, ring, rows};
+    drop_graphs(h);
+    return build_maps(h);
 }
 
 extern "C" int fvm_get_tune(fvm_handle *h, int *nt, int *ring, int *rows) {

@@ -230,6 +230,13 @@ int fvm_kernel_times(fvm_handle *h, fvm_kernel_time *out, int cap, int *count_ou
 int fvm_autotune(fvm_handle *h, const fvm_sim_params *p, int steps, float *best_ms_out);
 /* The launch tuning in use. */
 int fvm_get_tune(fvm_handle *h, int *nt, int *ring, int *rows);
+/* Pin a launch tuning (e.g. one an earlier fvm_autotune chose): threads per
+ * CTA 128 or 256, ring depth 4 or 6 rows, an even number of rows per CTA in
+ * 4..65536.  Results are bitwise the same under every allowed tuning; only the
+ * speed differs.  (Tiles start on even rows, so a row always takes the same
+ * place in the row pair the kernels evaluate together; the two places are
+ * separately compiled code and may round differently in the last bit.) */
+int fvm_set_tune(fvm_handle *h, int nt, int ring, int rows);
 
 /* ------------------------------------------------------------ batches
  * Many independent solves (different grids, Mach numbers, obstacles, Euler

@@ -842,6 +842,42 @@ extern "C" int fvm_read_fields(fvm_handle *h, float *rho, float *rho_u, float *r
     return FVM_OK;
 }
 
+static int check_region(const fvm_handle *h, int i0, int j0, int w, int hgt) {
+    if (i0 < 0 || j0 < 0 || w <= 0 || hgt <= 0 || (long long)i0 + w > h->g.nx || (long long)j0 + hgt > h->g.ny)
+        return set_err(FVM_ERR_INVALID, "region [%d, %d) x [%d, %d) outside the %d x %d grid", i0, i0 + w, j0, j0 + hgt,
+                       h->g.nx, h->g.ny);
+    return FVM_OK;
+}
+
+extern "C" int fvm_read_region(fvm_handle *h, int i0, int j0, int w, int hgt, float *rho, float *rho_u,
+                               float *rho_v, float *E, float *rho_e) {
+    CHECK_INIT(h);
+    if (int r = check_region(h, i0, j0, w, hgt)) return r;
+    float *dst[5] = {rho, rho_u, rho_v, E, rho_e};
+    const size_t off = (size_t)j0 * h->g.pitch + i0;
+    for (int k = 0; k < 5; k++) {
+        if (!dst[k]) continue;
+        CK(cudaMemcpy2DAsync(dst[k], (size_t)w * 4, h->Un + (size_t)k * h->g.plane + off, (size_t)h->g.pitch * 4,
+                             (size_t)w * 4, hgt, cudaMemcpyDeviceToHost, h->stream));
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    return FVM_OK;
+}
+
+extern "C" int fvm_read_region_geometry(fvm_handle *h, int i0, int j0, int w, int hgt, float *sdf,
+                                        uint8_t *cell_types) {
+    CHECK_INIT(h);
+    if (int r = check_region(h, i0, j0, w, hgt)) return r;
+    if (sdf)
+        CK(cudaMemcpy2DAsync(sdf, (size_t)w * 4, h->sdf + (size_t)j0 * h->g.pitch + i0, (size_t)h->g.pitch * 4,
+                             (size_t)w * 4, hgt, cudaMemcpyDeviceToHost, h->stream));
+    if (cell_types)
+        CK(cudaMemcpy2DAsync(cell_types, (size_t)w, h->ct + (size_t)j0 * h->g.nx + i0, (size_t)h->g.nx, (size_t)w,
+                             hgt, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return FVM_OK;
+}
+
 extern "C" int fvm_write_fields(fvm_handle *h, const float *rho, const float *rho_u, const float *rho_v,
                                 const float *E, const float *rho_e) {
     CHECK_INIT(h);
@@ -1121,10 +1157,18 @@ int fvm_internal_set_error(int code, const char *msg) { return set_err(code, "%s
 
 extern "C" int fvm_debug_ghost_table(fvm_handle *h, int *out, int cap, int *count_out) {
     CHECK_INIT(h);
-    static_assert(sizeof(GhostInfo) == 7 * sizeof(int), "GhostInfo layout");
+    static_assert(sizeof(GhostInfo) == 6 * sizeof(int), "GhostInfo layout");
     if (count_out) *count_out = h->n_ghost;
     int n = std::min(cap, h->n_ghost);
-    if (out && n > 0) CK(cudaMemcpy(out, h->ghosts, (size_t)n * sizeof(GhostInfo), cudaMemcpyDeviceToHost));
+    if (out && n > 0) {
+        std::vector<GhostInfo> t((size_t)n);
+        CK(cudaMemcpy(t.data(), h->ghosts, (size_t)n * sizeof(GhostInfo), cudaMemcpyDeviceToHost));
+        for (int k = 0; k < n; k++) {
+            int *o = out + (size_t)k * 7;
+            o[0] = (int)((long long)t[k].j * h->g.pitch + t[k].i);
+            memcpy(o + 1, &t[k], sizeof(GhostInfo));
+        }
+    }
     return FVM_OK;
 }
 

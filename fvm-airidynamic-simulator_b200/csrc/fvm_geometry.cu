@@ -314,7 +314,6 @@ __global__ void k_ghost_table(GridDesc g, const float *sdf, const uint8_t *ct, G
     uint32_t cand = 0;
     for (int k = 0; k < n; k++) cand |= (uint32_t)codes[k] << (4 * k);
     GhostInfo gi;
-    gi.pidx = (int)c;
     gi.i = i;
     gi.j = j;
     gi.gx = gx;

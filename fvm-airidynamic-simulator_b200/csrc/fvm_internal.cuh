@@ -28,8 +28,7 @@ struct GridDesc {
 // Candidate nibble k: bits 0-2 neighbour code in the reference order
 // {(-1,0),(1,0),(0,-1),(0,1),(-1,-1),(1,-1),(-1,1),(1,1)}, bit 3 set when the
 // neighbour is itself a ghost cell.
-struct GhostInfo {
-    int pidx;
+struct GhostInfo {  // the pitched index is j * pitch + i, formed in 64 bits where used
     int i, j;
     float gx, gy;
     uint32_t cand;

@@ -816,6 +816,7 @@ __device__ __forceinline__ void ghost_chunk(const GhostArgs &a, int first, int c
     if ((int)threadIdx.x >= count || k >= a.n) return;
     const GhostInfo gi = a.list[k];
     const long long plane = a.g.plane;
+    const long long pidx = (long long)gi.j * a.g.pitch + gi.i;
     long long best = -1;
     bool best_gh = false;
     for (int m = 0; m < gi.count; m++) {
@@ -824,7 +825,7 @@ __device__ __forceinline__ void ghost_chunk(const GhostArgs &a, int first, int c
         const bool gh = (code & 8) != 0;
         int di, dj;
         ghost_neighbour(d, di, dj);
-        const long long q = (long long)gi.pidx + di + (long long)dj * a.g.pitch;
+        const long long q = pidx + di + (long long)dj * a.g.pitch;
         const float rq = gh ? pre_bc(a, q, 0) : a.A[q];
         if (rq >= MIN_DENSITY) {
             best = q;
@@ -847,15 +848,15 @@ __device__ __forceinline__ void ghost_chunk(const GhostArgs &a, int first, int c
         ghost_state(s[0], s[1], s[2], s[3], gi.gx, gi.gy, a.wall, out);
     }
 #pragma unroll
-    for (int f = 0; f < 5; f++) a.A[f * plane + gi.pidx] = out[f];
+    for (int f = 0; f < 5; f++) a.A[f * plane + pidx] = out[f];
     if (a.cfl) {
         float uu, vv, pp, TT;
         prim_from_cons(out[0], out[1], out[2], out[3], out[4], uu, vv, pp, TT);
         ls = wave_speed(uu, vv, pp, out[0]);
         if (a.cfl == 2) {
             float pu, pv, ppp, pT;
-            prim_from_cons(pre_bc(a, gi.pidx, 0), pre_bc(a, gi.pidx, 1), pre_bc(a, gi.pidx, 2), pre_bc(a, gi.pidx, 3),
-                           pre_bc(a, gi.pidx, 4), pu, pv, ppp, pT);
+            prim_from_cons(pre_bc(a, pidx, 0), pre_bc(a, pidx, 1), pre_bc(a, pidx, 2), pre_bc(a, pidx, 3),
+                           pre_bc(a, pidx, 4), pu, pv, ppp, pT);
             ln = sutherland_mu(pT) / (out[0] + 1e-10f);
         }
     }

@@ -25,6 +25,7 @@ EXPORTS = [
     "fvm_create", "fvm_destroy", "fvm_set_stream", "fvm_initialize", "fvm_resize", "fvm_reset",
     "fvm_update_obstacle", "fvm_set_ext", "fvm_step", "fvm_steps", "fvm_compute_dt", "fvm_queue_dt",
     "fvm_read_dt", "fvm_synchronize", "fvm_get_cell_types", "fvm_get_sdf", "fvm_read_fields",
+    "fvm_read_region", "fvm_read_region_geometry",
     "fvm_write_fields", "fvm_read_primitives", "fvm_field_to_device", "fvm_cell_types_to_device",
     "fvm_vector_arrows", "fvm_max_temperature", "fvm_max_mach", "fvm_memory_usage", "fvm_gpu_mem_info",
     "fvm_diagnostics", "fvm_shock_standoff", "fvm_set_kernel_timing", "fvm_kernel_times",
@@ -84,6 +85,8 @@ def load_library(path=None):
     lib.fvm_get_cell_types.argtypes = [vp, vp]
     lib.fvm_get_sdf.argtypes = [vp, vp]
     lib.fvm_read_fields.argtypes = [vp] + [vp] * 5
+    lib.fvm_read_region.argtypes = [vp, i, i, i, i] + [vp] * 5
+    lib.fvm_read_region_geometry.argtypes = [vp, i, i, i, i, vp, vp]
     lib.fvm_write_fields.argtypes = [vp] + [vp] * 5
     lib.fvm_read_primitives.argtypes = [vp] + [vp] * 4
     lib.fvm_field_to_device.argtypes = [vp, i, vp]
@@ -225,6 +228,19 @@ class Solver:
         out = [np.empty(n, np.float32) for _ in range(5)]
         _check(self.lib.fvm_read_fields(self.h, *[_p(a) for a in out]))
         return np.stack([a.reshape(self.shape) for a in out])
+
+    def read_region(self, i0, j0, w, h):
+        """Conserved fields of the window [i0, i0+w) x [j0, j0+h): (5, h, w) float32."""
+        out = [np.empty(w * h, np.float32) for _ in range(5)]
+        _check(self.lib.fvm_read_region(self.h, int(i0), int(j0), int(w), int(h), *[_p(a) for a in out]))
+        return np.stack([a.reshape(h, w) for a in out])
+
+    def read_region_geometry(self, i0, j0, w, h):
+        """(sdf float32 (h, w), cell classes uint8 (h, w)) of the window."""
+        sdf = np.empty(w * h, np.float32)
+        ct = np.empty(w * h, np.uint8)
+        _check(self.lib.fvm_read_region_geometry(self.h, int(i0), int(j0), int(w), int(h), _p(sdf), _p(ct)))
+        return sdf.reshape(h, w), ct.reshape(h, w)
 
     def write_fields(self, U):
         U = [np.ascontiguousarray(U[k], dtype=np.float32).reshape(-1) for k in range(5)]

@@ -158,6 +158,14 @@ int fvm_get_sdf(fvm_handle *h, float *host_sdf);
  * its private d_rho_ ... d_rho_e_, src/include/solver.cuh:92-96).  Any pointer
  * may be NULL to skip that field.  fvm_write_fields recomputes primitives. */
 int fvm_read_fields(fvm_handle *h, float *rho, float *rho_u, float *rho_v, float *E, float *rho_e);
+/* The [i0, i0+w) x [j0, j0+hgt) window of the conserved fields into host
+ * arrays of w*hgt floats (row-major; NULL skips a field), for probes and
+ * windows of grids too large to copy whole.  No reference counterpart. */
+int fvm_read_region(fvm_handle *h, int i0, int j0, int w, int hgt, float *rho, float *rho_u, float *rho_v, float *E,
+                    float *rho_e);
+/* The same window of the signed distance field (w*hgt floats) and of the
+ * cell classes (w*hgt bytes, getCellTypes encoding); either may be NULL. */
+int fvm_read_region_geometry(fvm_handle *h, int i0, int j0, int w, int hgt, float *sdf, uint8_t *cell_types);
 int fvm_write_fields(fvm_handle *h, const float *rho, const float *rho_u, const float *rho_v,
                      const float *E, const float *rho_e);
 /* Primitive fields u, v, p, T as left by the last step/reset (host). */
@@ -403,8 +411,9 @@ int fvm_launch_count(fvm_handle *h, long long *count_out);
 int fvm_debug_stage1(fvm_handle *h, float dt, int with_ghost, float *rho, float *rho_u, float *rho_v, float *E,
                      float *rho_e);
 
-/* Test hook: copy the ghost-cell table (7 ints per ghost cell: pitched index,
- * i, j, normal x and y as float bits, packed candidate codes, count) to
+/* Test hook: copy the ghost-cell table (7 ints per ghost cell: pitched index
+ * j*pitch+i (grids below 2^31 cells), i, j, normal x and y as float bits,
+ * packed candidate codes, count) to
  * `out` (cap entries); *count_out receives the number of ghost cells. */
 int fvm_debug_ghost_table(fvm_handle *h, int *out, int cap, int *count_out);
 

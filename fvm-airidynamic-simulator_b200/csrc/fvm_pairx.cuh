@@ -1,5 +1,6 @@
-// fvm_pairx.cuh -- the two x-faces a stage-kernel thread evaluates per step
-// (same column, rows r and r+1) in packed FP32x2 arithmetic.
+// fvm_pairx.cuh -- the faces a stage-kernel thread evaluates per step in
+// packed FP32x2 arithmetic: the two x-faces (same column, rows r and r+1)
+// and the two y-faces (r-2 | r-1) and (r-1 | r).
 //
 // sm_100 issues two FP32 adds, multiplies or FMAs per instruction
 // (__fadd2_rn / __fmul2_rn / __ffma2_rn) at the same FMA throughput as the
@@ -7,13 +8,15 @@
 // are bound by.  The primitive ring stores each row pair interleaved, {rho_r,
 // rho_r+1, u_r, u_r+1} and {v_r, v_r+1, p_r, p_r+1}, so one shared-memory
 // vector load yields both rows' operands as aligned register pairs and no
-// register moves are needed; lane .x is row r, lane .y row r+1.  Square
-// roots, reciprocals, min/max and the wave-fan selections stay per lane.
+// register moves are needed; lane .x is row r, lane .y row r+1.  The y-faces'
+// upper cells straddle two row pairs and are paired from those loads.
+// Square roots, reciprocals, min/max and the wave-fan selections stay per
+// lane.
 //
-// The arithmetic is face_flux_sl + hllc_flux for an x-face (fvm_math.cuh;
-// reference computeFluxesKernel, src/solver.cu:1502-1598, and its HLLC,
-// :1112-1223) with explicit fused multiply-adds, so results can differ from
-// the scalar form in the last bits.
+// The arithmetic is face_flux_sl + hllc_flux (fvm_math.cuh; reference
+// computeFluxesKernel, src/solver.cu:1502-1598 / :1601-1682, and its HLLC,
+// :1112-1223 / :1315-1430) with explicit fused multiply-adds, so results can
+// differ from the scalar form in the last bits.
 #pragma once
 #include "fvm_math.cuh"
 
@@ -59,45 +62,47 @@ __device__ __forceinline__ PairPrim pair_prim(const float4 &A, const float4 &B) 
     return PairPrim{mk2(A.x, A.y), mk2(A.z, A.w), mk2(B.x, B.y), mk2(B.z, B.w)};
 }
 
-// x-faces of rows r (lane .x -> f0) and r+1 (lane .y -> f1) between cells
-// a | b, stencil m1, a, b, p2; out = {mass, x-momentum, y-momentum, energy,
-// rho_e}.  valid*: neither side a wall; near*: first order (wall at m1/p2).
-template <int SCHEME, int LIM>
-__device__ __forceinline__ void face_pair_x(bool valid0, bool near0, bool valid1, bool near1, const PairPrim &m1,
-                                            const PairPrim &a, const PairPrim &b, const PairPrim &p2, float f0[5],
-                                            float f1[5]) {
-    if (SCHEME != 0) {  // AUSM+: per lane through the scalar path
-        face_flux<true, SCHEME, LIM>(valid0, near0, Prim{m1.rho.x, m1.u.x, m1.v.x, m1.p.x},
-                                     Prim{a.rho.x, a.u.x, a.v.x, a.p.x}, Prim{b.rho.x, b.u.x, b.v.x, b.p.x},
-                                     Prim{p2.rho.x, p2.u.x, p2.v.x, p2.p.x}, f0);
-        face_flux<true, SCHEME, LIM>(valid1, near1, Prim{m1.rho.y, m1.u.y, m1.v.y, m1.p.y},
-                                     Prim{a.rho.y, a.u.y, a.v.y, a.p.y}, Prim{b.rho.y, b.u.y, b.v.y, b.p.y},
-                                     Prim{p2.rho.y, p2.u.y, p2.v.y, p2.p.y}, f1);
-        return;
-    }
+// Limited slopes of a cell pair in the face frame: normal and tangential
+// velocity components (x-faces: u, v; y-faces: v, u).
+struct PairSl {
+    f2 rho, n, t, p;
+};
+
+// Two faces between cells a | b (lane .x -> f0, lane .y -> f1) from the
+// cells' primitives and limited slopes sa, sb (face frame); out = {mass,
+// x-momentum, y-momentum, energy, rho_e}.  valid*: neither side a wall;
+// near*: first order (wall at the outer stencil cells).
+template <bool XDIR>
+__device__ __forceinline__ void face_pair_core(bool valid0, bool near0, bool valid1, bool near1, const PairPrim &a,
+                                               const PairSl &sa, const PairPrim &b, const PairSl &sb, float f0[5],
+                                               float f1[5]) {
     const bool fo0 = near0 || a.rho.x < LOW_DENSITY || b.rho.x < LOW_DENSITY;
     const bool fo1 = near1 || a.rho.y < LOW_DENSITY || b.rho.y < LOW_DENSITY;
     const f2 hp = splat(0.5f);
     const f2 omh = mk2(fo0 ? 0.0f : 0.5f, fo1 ? 0.0f : 0.5f);  // half order mask
+    const f2 an = XDIR ? a.u : a.v, at = XDIR ? a.v : a.u;
+    const f2 bn = XDIR ? b.u : b.v, bt = XDIR ? b.v : b.u;
     // MUSCL: left = a + slope_a/2, right = b - slope_b/2
-    f2 rL = p_fma(p_slope<LIM>(m1.rho, a.rho, b.rho), omh, a.rho);
-    const f2 nL = p_fma(p_slope<LIM>(m1.u, a.u, b.u), omh, a.u);
-    const f2 tL = p_fma(p_slope<LIM>(m1.v, a.v, b.v), omh, a.v);
-    f2 pL = p_fma(p_slope<LIM>(m1.p, a.p, b.p), omh, a.p);
+    f2 rL = p_fma(sa.rho, omh, a.rho);
+    const f2 nL = p_fma(sa.n, omh, an);
+    const f2 tL = p_fma(sa.t, omh, at);
+    f2 pL = p_fma(sa.p, omh, a.p);
     const f2 omm = mk2(-omh.x, -omh.y);
-    f2 rR = p_fma(p_slope<LIM>(a.rho, b.rho, p2.rho), omm, b.rho);
-    const f2 nR = p_fma(p_slope<LIM>(a.u, b.u, p2.u), omm, b.u);
-    const f2 tR = p_fma(p_slope<LIM>(a.v, b.v, p2.v), omm, b.v);
-    f2 pR = p_fma(p_slope<LIM>(a.p, b.p, p2.p), omm, b.p);
+    f2 rR = p_fma(sb.rho, omm, b.rho);
+    const f2 nR = p_fma(sb.n, omm, bn);
+    const f2 tR = p_fma(sb.t, omm, bt);
+    f2 pR = p_fma(sb.p, omm, b.p);
     rL = p_max(rL, MIN_DENSITY);
     pL = p_max(pL, MIN_PRESSURE);
     rR = p_max(rR, MIN_DENSITY);
     pR = p_max(pR, MIN_PRESSURE);
-    // E = p/(gamma-1) + rho*(u^2 + v^2)/2
+    // E = p/(gamma-1) + rho*(u^2 + v^2)/2, the x component squared first
     const f2 igm1 = splat(1.0f / (GAMMA - 1.0f));
     const f2 eL = p_mul(pL, igm1), eR = p_mul(pR, igm1);
-    const f2 EL = p_fma(p_mul(hp, rL), p_fma(nL, nL, p_mul(tL, tL)), eL);
-    const f2 ER = p_fma(p_mul(hp, rR), p_fma(nR, nR, p_mul(tR, tR)), eR);
+    const f2 qL = XDIR ? p_fma(nL, nL, p_mul(tL, tL)) : p_fma(tL, tL, p_mul(nL, nL));
+    const f2 qR = XDIR ? p_fma(nR, nR, p_mul(tR, tR)) : p_fma(tR, tR, p_mul(nR, nR));
+    const f2 EL = p_fma(p_mul(hp, rL), qL, eL);
+    const f2 ER = p_fma(p_mul(hp, rR), qR, eR);
 
     // ---- HLLC with Roe-averaged Davis wave speeds
     const f2 cL = p_sqrt(p_div(p_mul(splat(GAMMA), pL), rL));
@@ -108,7 +113,8 @@ __device__ __forceinline__ void face_pair_x(bool valid0, bool near0, bool valid1
     const f2 ut_roe = p_div(p_fma(sqL, tL, p_mul(sqR, tR)), den);
     const f2 HL = p_div(p_add(EL, pL), rL), HR = p_div(p_add(ER, pR), rR);
     const f2 H_roe = p_div(p_fma(sqL, HL, p_mul(sqR, HR)), den);
-    const f2 c2 = p_mul(splat(GAMMA - 1.0f), p_fma(splat(-0.5f), p_fma(un_roe, un_roe, p_mul(ut_roe, ut_roe)), H_roe));
+    const f2 q_roe = XDIR ? p_fma(un_roe, un_roe, p_mul(ut_roe, ut_roe)) : p_fma(ut_roe, ut_roe, p_mul(un_roe, un_roe));
+    const f2 c2 = p_mul(splat(GAMMA - 1.0f), p_fma(splat(-0.5f), q_roe, H_roe));
     const f2 c_avg = p_mul(hp, p_add(cL, cR));
     const f2 c_roe = mk2(c2.x > 0.0f ? sqrtf(c2.x) : c_avg.x, c2.y > 0.0f ? sqrtf(c2.y) : c_avg.y);
     f2 SL = p_min(p_sub(nL, cL), p_sub(un_roe, c_roe));
@@ -131,7 +137,7 @@ __device__ __forceinline__ void face_pair_x(bool valid0, bool near0, bool valid1
     const f2 rkd = p_mul(rK, d);  // rK (SK - unK): the same product as mL / mR
     const f2 fK0 = p_mul(rK, nK);
     const f2 fK1 = p_fma(fK0, nK, pK);
-    const f2 fK2 = p_mul(fK0, tK);
+    const f2 fK2 = XDIR ? p_mul(fK0, tK) : p_mul(p_mul(rK, tK), nK);  // (rho u) v either way
     const f2 fK3 = p_mul(p_add(EK, pK), nK);
     f2 cd = p_sub(SK, Ss);
     cd = mk2(fabsf(cd.x) < 1e-10f ? (cd.x >= 0.0f ? 1e-10f : -1e-10f) : cd.x,
@@ -147,17 +153,70 @@ __device__ __forceinline__ void face_pair_x(bool valid0, bool near0, bool valid1
     // upwinded internal-energy flux
     const f2 uf = p_add(nL, nR);  // sign of 0.5 (unL + unR)
     const f2 F4 = p_sel(uf.x >= 0.0f, uf.y >= 0.0f, p_mul(eL, nL), p_mul(eR, nR));
-    // wall faces: no mass/energy flux, x-momentum flux = pressure of the left cell
+    const f2 Fx = XDIR ? Fn : Ft, Fy = XDIR ? Ft : Fn;
+    // wall faces: no mass/energy flux, normal momentum flux = pressure of the left/bottom cell
     f0[0] = valid0 ? F0.x : 0.0f;
-    f0[1] = valid0 ? Fn.x : a.p.x;
-    f0[2] = valid0 ? Ft.x : 0.0f;
+    f0[1] = valid0 ? Fx.x : (XDIR ? a.p.x : 0.0f);
+    f0[2] = valid0 ? Fy.x : (XDIR ? 0.0f : a.p.x);
     f0[3] = valid0 ? F3.x : 0.0f;
     f0[4] = valid0 ? F4.x : 0.0f;
     f1[0] = valid1 ? F0.y : 0.0f;
-    f1[1] = valid1 ? Fn.y : a.p.y;
-    f1[2] = valid1 ? Ft.y : 0.0f;
+    f1[1] = valid1 ? Fx.y : (XDIR ? a.p.y : 0.0f);
+    f1[2] = valid1 ? Fy.y : (XDIR ? 0.0f : a.p.y);
     f1[3] = valid1 ? F3.y : 0.0f;
     f1[4] = valid1 ? F4.y : 0.0f;
+}
+
+// x-faces of rows r (lane .x -> f0) and r+1 (lane .y -> f1) between cells
+// a | b, stencil m1, a, b, p2.
+template <int SCHEME, int LIM>
+__device__ __forceinline__ void face_pair_x(bool valid0, bool near0, bool valid1, bool near1, const PairPrim &m1,
+                                            const PairPrim &a, const PairPrim &b, const PairPrim &p2, float f0[5],
+                                            float f1[5]) {
+    if (SCHEME != 0) {  // AUSM+: per lane through the scalar path
+        face_flux<true, SCHEME, LIM>(valid0, near0, Prim{m1.rho.x, m1.u.x, m1.v.x, m1.p.x},
+                                     Prim{a.rho.x, a.u.x, a.v.x, a.p.x}, Prim{b.rho.x, b.u.x, b.v.x, b.p.x},
+                                     Prim{p2.rho.x, p2.u.x, p2.v.x, p2.p.x}, f0);
+        face_flux<true, SCHEME, LIM>(valid1, near1, Prim{m1.rho.y, m1.u.y, m1.v.y, m1.p.y},
+                                     Prim{a.rho.y, a.u.y, a.v.y, a.p.y}, Prim{b.rho.y, b.u.y, b.v.y, b.p.y},
+                                     Prim{p2.rho.y, p2.u.y, p2.v.y, p2.p.y}, f1);
+        return;
+    }
+    const PairSl sa{p_slope<LIM>(m1.rho, a.rho, b.rho), p_slope<LIM>(m1.u, a.u, b.u), p_slope<LIM>(m1.v, a.v, b.v),
+                    p_slope<LIM>(m1.p, a.p, b.p)};
+    const PairSl sb{p_slope<LIM>(a.rho, b.rho, p2.rho), p_slope<LIM>(a.u, b.u, p2.u), p_slope<LIM>(a.v, b.v, p2.v),
+                    p_slope<LIM>(a.p, b.p, p2.p)};
+    face_pair_core<true>(valid0, near0, valid1, near1, a, sa, b, sb, f0, f1);
+}
+
+// The two y-faces a stage-kernel thread evaluates per step, (r-2 | r-1) in
+// lane .x -> f0 and (r-1 | r) in lane .y -> f1, from the primitives of rows
+// (r-2, r-1) = lo, (r-1, r) = mid and (r, r+1) = hi of one column and the
+// y-slopes of row r-2 (carried from the previous step; `sy_lo` in, the slopes
+// of row r out for the next step).
+template <int SCHEME, int LIM>
+__device__ __forceinline__ void face_pair_y(bool valid0, bool near0, bool valid1, bool near1, const PairPrim &lo,
+                                            const PairPrim &mid, const PairPrim &hi, float sy_lo[4], float f0[5],
+                                            float f1[5]) {
+    // slopes of rows (r-1, r): limited(row-1, row, row+1), face frame (v normal, u tangential)
+    const PairSl sm{p_slope<LIM>(lo.rho, mid.rho, hi.rho), p_slope<LIM>(lo.v, mid.v, hi.v),
+                    p_slope<LIM>(lo.u, mid.u, hi.u), p_slope<LIM>(lo.p, mid.p, hi.p)};
+    // slopes of rows (r-2, r-1)
+    const PairSl sl{mk2(sy_lo[0], sm.rho.x), mk2(sy_lo[1], sm.n.x), mk2(sy_lo[2], sm.t.x), mk2(sy_lo[3], sm.p.x)};
+    if (SCHEME != 0) {  // AUSM+: per lane through the scalar path
+        const float sa0[4] = {sl.rho.x, sl.n.x, sl.t.x, sl.p.x}, sb0[4] = {sm.rho.x, sm.n.x, sm.t.x, sm.p.x};
+        const float sb1[4] = {sm.rho.y, sm.n.y, sm.t.y, sm.p.y};
+        face_flux_sl<false, SCHEME>(valid0, near0, Prim{lo.rho.x, lo.u.x, lo.v.x, lo.p.x}, sa0,
+                                    Prim{mid.rho.x, mid.u.x, mid.v.x, mid.p.x}, sb0, f0);
+        face_flux_sl<false, SCHEME>(valid1, near1, Prim{lo.rho.y, lo.u.y, lo.v.y, lo.p.y}, sb0,
+                                    Prim{mid.rho.y, mid.u.y, mid.v.y, mid.p.y}, sb1, f1);
+    } else {
+        face_pair_core<false>(valid0, near0, valid1, near1, lo, sl, mid, sm, f0, f1);
+    }
+    sy_lo[0] = sm.rho.y;
+    sy_lo[1] = sm.n.y;
+    sy_lo[2] = sm.t.y;
+    sy_lo[3] = sm.p.y;
 }
 
 }  // namespace fvm

@@ -237,32 +237,25 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
             break;
         }
         // ---- phase 2: y-faces of column cy, then the update of rows r-2, r-1
-        float4 c3, c2, c1, c0, cp;  // column cy, rows r-3 .. r+1 as (rho, u, v, p)
-        {
-            const float4 A2 = PA[s2 * NT + cy], B2 = PB[s2 * NT + cy];
-            const float4 A1 = PA[s1 * NT + cy], B1 = PB[s1 * NT + cy];
-            const float4 A0 = PA[s0 * NT + cy], B0 = PB[s0 * NT + cy];
-            c3 = make_float4(A2.y, A2.w, B2.y, B2.w);
-            c2 = make_float4(A1.x, A1.z, B1.x, B1.z);
-            c1 = make_float4(A1.y, A1.w, B1.y, B1.w);
-            c0 = make_float4(A0.x, A0.z, B0.x, B0.z);
-            cp = make_float4(A0.y, A0.w, B0.y, B0.w);
-        }
+        // column cy, rows r-3 .. r: pairs q-2 (rows r-4, r-3), q-1 (r-2, r-1), q (r, r+1)
+        const float4 A1 = PA[s1 * NT + cy], B1 = PB[s1 * NT + cy];
+        const float4 A0 = PA[s0 * NT + cy], B0 = PB[s0 * NT + cy];
+        const float rho3 = PA[s2 * NT + cy].y;                       // density of row r-3
+        const float4 c2 = make_float4(A1.x, A1.z, B1.x, B1.z);        // row r-2 (rho, u, v, p)
+        const float4 c1 = make_float4(A1.y, A1.w, B1.y, B1.w);        // row r-1
+        const float rho0 = A0.x;                                      // density of row r
         // densities of rows r-2, r-1 beside column cy
         const float2 rhoE = *reinterpret_cast<const float2 *>(&PA[s1 * NT + cy + 1]);
         const float2 rhoW = *reinterpret_cast<const float2 *>(&PA[s1 * NT + cy - 1]);
         float fy0[5], fy1[5];
         {
+            // y-faces (r-2 | r-1) and (r-1 | r) as one lane pair; the y-slopes
+            // of row r-2 are those of row r in step q-1
             const uint32_t my0 = M[pc1 * NT + cy], my1 = M[(pc1 + 1) * NT + cy];
-            // y-slopes of rows r-1 and r; those of row r-2 are row r of step q-1
-            const Prim q2{c2.x, c2.y, c2.z, c2.w}, q1{c1.x, c1.y, c1.z, c1.w}, q0{c0.x, c0.y, c0.z, c0.w};
-            float s1[4], s0[4];
-            cell_slopes<false, LIM>(q2, q1, q0, s1);
-            cell_slopes<false, LIM>(q1, q0, Prim{cp.x, cp.y, cp.z, cp.w}, s0);
-            face_flux_sl<false, SCHEME>((my0 & MB_YV) != 0, (my0 & MB_YN) != 0, q2, sy2, q1, s1, fy0);
-            face_flux_sl<false, SCHEME>((my1 & MB_YV) != 0, (my1 & MB_YN) != 0, q1, s1, q0, s0, fy1);
-#pragma unroll
-            for (int k = 0; k < 4; k++) sy2[k] = s0[k];
+            const PairPrim lo = pair_prim(A1, B1), hi = pair_prim(A0, B0);
+            const PairPrim mid{mk2(A1.y, A0.x), mk2(A1.w, A0.z), mk2(B1.y, B0.x), mk2(B1.w, B0.z)};
+            face_pair_y<SCHEME, LIM>((my0 & MB_YV) != 0, (my0 & MB_YN) != 0, (my1 & MB_YV) != 0, (my1 & MB_YN) != 0,
+                                     lo, mid, hi, sy2, fy0, fy1);
         }
 #pragma unroll
         for (int h = 0; h < 2; h++) {
@@ -288,8 +281,8 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
                     }
                     const float4 pc = h ? c1 : c2;
                     const float rxR = h ? rhoE.y : rhoE.x, rxL = h ? rhoW.y : rhoW.x;
-                    const float ryT = h ? c0.x : c1.x;
-                    const float ryB = h ? c2.x : c3.x;
+                    const float ryT = h ? rho0 : c1.x;
+                    const float ryB = h ? c2.x : rho3;
                     const bool edge_y = (urow == 0 || urow == ny - 1);
                     update_cell(Uc, fR, fL, fT, fB, rxR, rxL, ryT, ryB, pc.w, edge_x, edge_y, !edge_x && !edge_y, ua,
                                 Un);

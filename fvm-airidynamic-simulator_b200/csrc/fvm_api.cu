@@ -1121,6 +1121,16 @@ extern "C" int fvm_set_tune(fvm_handle *h, int nt, int ring, int rows) {
     return build_maps(h);
 }
 
+extern "C" int fvm_nonfinite_count(fvm_handle *h, unsigned long long *count, int reset) {
+    CHECK_INIT(h);
+    unsigned v = 0;
+    CK(cudaMemcpyAsync(&v, &h->sc->nonfinite, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
+    if (reset) CK(cudaMemsetAsync(&h->sc->nonfinite, 0, sizeof(unsigned), h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (count) *count = v;
+    return FVM_OK;
+}
+
 extern "C" int fvm_get_tune(fvm_handle *h, int *nt, int *ring, int *rows) {
     CHECK_INIT(h);
     if (nt) *nt = h->tune.nt;

@@ -50,6 +50,21 @@ __device__ __forceinline__ void block_max2_publish(float a, float b, float *dst)
     }
 }
 
+// CFL maxima of the block plus the number of non-finite cells its threads
+// saw (one atomic per warp that saw any); every thread of the block calls it.
+template <int NT>
+__device__ __forceinline__ void block_publish(float a, float b, unsigned bad, DevScalars *sc) {
+    block_max2_publish<NT>(a, b, sc->red);
+    bad = __reduce_add_sync(0xffffffffu, bad);
+    if ((threadIdx.x & 31) == 0 && bad) atomicAdd(&sc->nonfinite, bad);
+}
+
+// A conserved state with a NaN or infinite field (their sum is then not
+// finite; finite states are far below the float range).
+__device__ __forceinline__ unsigned nonfinite5(const float U[5]) {
+    return isfinite(U[0] + U[1] + U[2] + U[3] + U[4]) ? 0u : 1u;
+}
+
 // Width of one TMA box of the halo'd input (a TMA box spans at most 256
 // elements per dimension; 132 floats = 528 B keeps every box start 16-byte
 // aligned).  A staged row is NB boxes, each stored as [field][kBox].
@@ -145,7 +160,8 @@ struct RingPos {
 // false when a bounded wait expired (error recorded; caller must stop).
 template <int NT, int K, int STAGE, int SCHEME, int LIM>
 __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUtensorMap *tm_blend, const StepArgs &a,
-                                           int i0, int j0, unsigned char *smem, RingPos &rp, float &lmax_speed) {
+                                           int i0, int j0, unsigned char *smem, RingPos &rp, float &lmax_speed,
+                                           unsigned &nbad) {
     using L = StageLayout<NT, K, STAGE>;
     constexpr int W = L::W, KP = L::KP;
     static_assert(L::PP == 3 && L::XP == 1 && KP >= 2, "ring sizes");
@@ -298,6 +314,7 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
                     float uu, vv, pp, TT;
                     prim_from_cons(Un[0], Un[1], Un[2], Un[3], Un[4], uu, vv, pp, TT);
                     lmax_speed = fmaxf(lmax_speed, wave_speed(uu, vv, pp, Un[0]));
+                    nbad += nonfinite5(Un);
                 }
                 float *dst = outp + (size_t)urow * g.pitch;
 #pragma unroll
@@ -370,10 +387,11 @@ __global__ void __launch_bounds__(NT, (STAGE == 1 ? 768 : 640) / NT)
     }
     RingPos rp{0};
     float lmax = 0.0f;
+    unsigned nbad = 0;
     if (!stage_tile<NT, K, STAGE, SCHEME, LIM>(&tm_in, &tm_blend, a, blockIdx.x * L::W, blockIdx.y * a.rows_per_cta,
-                                               smem, rp, lmax))
+                                               smem, rp, lmax, nbad))
         return;
-    if (a.cfl) block_max2_publish<NT>(lmax, 0.0f, a.sc->red);
+    if (a.cfl) block_publish<NT>(lmax, 0.0f, nbad, a.sc);
 }
 
 template <int NT, int K>
@@ -414,7 +432,8 @@ struct ViscLayout {
 // by selects and predicated stores), so their dependency chains interleave.
 template <int NT, int K>
 __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const StepArgs &a, int i0, int j0,
-                                             unsigned char *smem, RingPos &rp, float &lmax_speed, float &lmax_nu) {
+                                             unsigned char *smem, RingPos &rp, float &lmax_speed, float &lmax_nu,
+                                             unsigned &nbad) {
     using L = ViscLayout<NT, K>;
     constexpr int KP = L::KP;
     static_assert(L::PP == 3 && L::TP == 2 && KP >= 2, "ring sizes");
@@ -604,6 +623,7 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
                     const bool counted = store[h] && ctype[h] != CT_GHOST;
                     const float ws = wave_speed(uu, vv, pp, U[h][0]);
                     lmax_speed = counted ? fmaxf(lmax_speed, ws) : lmax_speed;
+                    nbad += counted ? nonfinite5(U[h]) : 0u;
                     if (a.cfl == 2) {
                         const float mu = (ctype[h] == CT_SOLID) ? 0.0f : P[(pc1 + h) * NT + tp].w;
                         const float nu = mu / (U[h][0] + 1e-10f);
@@ -658,8 +678,10 @@ __global__ void __launch_bounds__(NT) k_viscous(const __grid_constant__ CUtensor
     }
     RingPos rp{0};
     float ls = 0.0f, ln = 0.0f;
-    if (!viscous_tile<NT, K>(&tm_in, a, blockIdx.x * L::W, blockIdx.y * a.rows_per_cta, smem, rp, ls, ln)) return;
-    if (a.cfl) block_max2_publish<NT>(ls, ln, a.sc->red);
+    unsigned nbad = 0;
+    if (!viscous_tile<NT, K>(&tm_in, a, blockIdx.x * L::W, blockIdx.y * a.rows_per_cta, smem, rp, ls, ln, nbad))
+        return;
+    if (a.cfl) block_publish<NT>(ls, ln, nbad, a.sc);
 }
 
 // --------------------------------------------------------- batched launches
@@ -730,10 +752,11 @@ __global__ void __launch_bounds__(NT, 640 / NT) k_stage_batch(const BatchInst *_
         if (threadIdx.x == 0) s_args = batch_args(I, out_role, bc, cfl, 1.0f, rows);
         __syncthreads();
         float lmax = 0.0f;
+        unsigned nbad = 0;
         if (!stage_tile<NT, K, STAGE, SCHEME, LIM>(&I.tm_in[role_buf(I, in_role)], &I.tm_ctr[role_buf(I, blend_role)],
-                                                   s_args, td.i0, td.j0, smem, rp, lmax))
+                                                   s_args, td.i0, td.j0, smem, rp, lmax, nbad))
             return;
-        if (cfl) block_max2_publish<NT>(lmax, 0.0f, I.sc->red);
+        if (cfl) block_publish<NT>(lmax, 0.0f, nbad, I.sc);
     }
 }
 
@@ -761,8 +784,10 @@ __global__ void __launch_bounds__(NT, 640 / NT) k_viscous_batch(const BatchInst 
         if (threadIdx.x == 0) s_args = batch_args(I, post ? ROLE_X : ROLE_D, post, post ? 2 : 0, 0.5f, rows);
         __syncthreads();
         float ls = 0.0f, ln = 0.0f;
-        if (!viscous_tile<NT, K>(&I.tm_in[role_buf(I, in_role)], s_args, td.i0, td.j0, smem, rp, ls, ln)) return;
-        if (post) block_max2_publish<NT>(ls, ln, I.sc->red);
+        unsigned nbad = 0;
+        if (!viscous_tile<NT, K>(&I.tm_in[role_buf(I, in_role)], s_args, td.i0, td.j0, smem, rp, ls, ln, nbad))
+            return;
+        if (post) block_publish<NT>(ls, ln, nbad, I.sc);
     }
 }
 
@@ -804,7 +829,8 @@ __device__ void finalize_cfl(const GhostArgs &a) {
 // ghost cells, whose pre-call value comes from B1/B2.  Handles table entries
 // [first, first + count) with this block's threads; returns the thread's CFL
 // contributions.
-__device__ __forceinline__ void ghost_chunk(const GhostArgs &a, int first, int count, float &ls, float &ln) {
+__device__ __forceinline__ void ghost_chunk(const GhostArgs &a, int first, int count, float &ls, float &ln,
+                                            unsigned &nbad) {
     const int k = first + (int)threadIdx.x;
     if ((int)threadIdx.x >= count || k >= a.n) return;
     const GhostInfo gi = a.list[k];
@@ -846,6 +872,7 @@ __device__ __forceinline__ void ghost_chunk(const GhostArgs &a, int first, int c
         float uu, vv, pp, TT;
         prim_from_cons(out[0], out[1], out[2], out[3], out[4], uu, vv, pp, TT);
         ls = wave_speed(uu, vv, pp, out[0]);
+        nbad = nonfinite5(out);
         if (a.cfl == 2) {
             float pu, pv, ppp, pT;
             prim_from_cons(pre_bc(a, pidx, 0), pre_bc(a, pidx, 1), pre_bc(a, pidx, 2), pre_bc(a, pidx, 3),
@@ -857,8 +884,9 @@ __device__ __forceinline__ void ghost_chunk(const GhostArgs &a, int first, int c
 
 // Reduce the block's CFL contributions and, for the last of `nblocks`
 // blocks of this solve, publish the step's maxima / next dt.
-__device__ __forceinline__ void ghost_publish(const GhostArgs &a, float ls, float ln, unsigned nblocks) {
-    if (a.cfl) block_max2_publish<128>(ls, ln, a.sc->red);
+__device__ __forceinline__ void ghost_publish(const GhostArgs &a, float ls, float ln, unsigned nbad,
+                                              unsigned nblocks) {
+    if (a.cfl) block_publish<128>(ls, ln, nbad, a.sc);
     if (a.finalize) {
         __shared__ bool last;
         __threadfence();
@@ -874,8 +902,9 @@ __device__ __forceinline__ void ghost_publish(const GhostArgs &a, float ls, floa
 
 __global__ void __launch_bounds__(128) k_ghost(const GhostArgs a) {
     float ls = 0.0f, ln = 0.0f;
-    ghost_chunk(a, blockIdx.x * 128, 128, ls, ln);
-    ghost_publish(a, ls, ln, gridDim.x);
+    unsigned nbad = 0;
+    ghost_chunk(a, blockIdx.x * 128, 128, ls, ln, nbad);
+    ghost_publish(a, ls, ln, nbad, gridDim.x);
 }
 
 // Batched ghost pass: one block per (instance, chunk of <=128 ghost cells).
@@ -912,8 +941,9 @@ __global__ void __launch_bounds__(128) k_ghost_batch(const BatchInst *__restrict
         a.flip_parity = 1;
     }
     float ls = 0.0f, ln = 0.0f;
-    ghost_chunk(a, ch.first, ch.count, ls, ln);
-    ghost_publish(a, ls, ln, (unsigned)I.n_gchunks);
+    unsigned nbad = 0;
+    ghost_chunk(a, ch.first, ch.count, ls, ln, nbad);
+    ghost_publish(a, ls, ln, nbad, (unsigned)I.n_gchunks);
 }
 
 // Phase-1 boundary conditions in place (set-up path).

@@ -35,7 +35,8 @@ EXPORTS = [
     "fvm_batch_instance_bytes", "fvm_batch_retire", "fvm_batch_trim", "fvm_server_create", "fvm_server_submit",
     "fvm_server_poll", "fvm_server_wait", "fvm_server_drain", "fvm_server_get_stats", "fvm_server_destroy",
     "fvm_state_max_noalloc", "fvm_shedding_stats", "fvm_colormap_to_device", "fvm_colormap_table",
-    "fvm_save_checkpoint", "fvm_load_checkpoint", "fvm_checkpoint_info", "fvm_autotune", "fvm_get_tune", "fvm_set_tune", "fvm_debug_stage1", "fvm_debug_ghost_table", "fvm_build_info",
+    "fvm_save_checkpoint", "fvm_load_checkpoint", "fvm_checkpoint_info", "fvm_autotune", "fvm_get_tune",
+    "fvm_set_tune", "fvm_nonfinite_count", "fvm_debug_stage1", "fvm_debug_ghost_table", "fvm_build_info",
 ]
 
 
@@ -137,6 +138,7 @@ def load_library(path=None):
     lib.fvm_server_destroy.argtypes = [vp]
     lib.fvm_get_tune.argtypes = [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i)]
     lib.fvm_set_tune.argtypes = [vp, i, i, i]
+    lib.fvm_nonfinite_count.argtypes = [vp, C.POINTER(C.c_ulonglong), i]
     lib.fvm_debug_ghost_table.argtypes = [vp, vp, i, C.POINTER(i)]
     _lib = lib
     return lib
@@ -345,6 +347,12 @@ class Solver:
         ms = C.c_float()
         _check(self.lib.fvm_autotune(self.h, C.byref(self.params), int(steps), C.byref(ms)))
         return ms.value
+
+    def nonfinite_count(self, reset=False):
+        """(cell, step) pairs that came out of a step non-finite (see fvm_nonfinite_count)."""
+        v = C.c_ulonglong()
+        _check(self.lib.fvm_nonfinite_count(self.h, C.byref(v), 1 if reset else 0))
+        return v.value
 
     def set_tune(self, threads, ring, rows):
         """Pin the launch tuning (see fvm_set_tune)."""

@@ -193,6 +193,14 @@ int fvm_vector_arrows(fvm_handle *h, float *dev_vertex_data, int max_vertices, i
 /* CFDSolver::getMaxTemperature / getMaxMach (src/solver.cu:3417-3426). */
 int fvm_max_temperature(fvm_handle *h, float *out);
 int fvm_max_mach(fvm_handle *h, float *out);
+/* Number of (cell, step) pairs whose state came out of a step with a NaN or
+ * infinite field, counted on the device inside the steps' CFL reductions
+ * since the solve was (re)initialised or the counter was last reset
+ * (reset != 0 clears it after reading).  The reference has no such check: its
+ * update rolls non-finite results back to the old value, which repairs most
+ * of them but not all (a non-finite input field, viscous terms).  No
+ * reference counterpart. */
+int fvm_nonfinite_count(fvm_handle *h, unsigned long long *count, int reset);
 /* CFDSolver::getSimulationMemoryUsage (src/solver.cu:3474-3514): bytes this handle holds. */
 int fvm_memory_usage(fvm_handle *h, size_t *bytes);
 /* CFDSolver::getGPUMemoryInfo (src/solver.cu:3468-3471): (free, total), the

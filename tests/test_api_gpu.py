@@ -270,3 +270,28 @@ def test_autotune_restores_state_and_caches_choice():
     s.step(6)
     s3, p3, _ = _solver("euler_m3_circle", 301, 150)
     assert np.isfinite(s.fields()).all()
+
+
+@pytest.mark.parametrize("name,field", [("euler_m3_circle", 1), ("ns_karman_re200", 1), ("ns_karman_re200", 3)])
+def test_nonfinite_cells_are_counted_on_the_device(name, field):
+    """A NaN written into one fluid cell is counted by the device-side check
+    fused into the steps' CFL reductions; a clean solve counts nothing, and
+    a reset clears the counter."""
+    clean, p, e = _solver(name)
+    p.dt = clean.compute_dt()
+    clean.step(10)
+    assert np.isfinite(clean.fields()).all()
+    assert clean.nonfinite_count() == 0
+    s, p, e = _solver(name)
+    p.dt = s.compute_dt()
+    U = s.fields()
+    ct = s.cell_types()
+    j, i = s.params.ny // 2, s.params.nx - 40
+    assert ct[j, i] == abi.CELL_FLUID
+    U[field, j, i] = np.nan
+    s.write_fields(U)
+    s.step(3)
+    n = s.nonfinite_count(reset=True)
+    bad = int((~np.isfinite(s.fields())).any(axis=0).sum())
+    assert n >= 1 and bad >= 1, (n, bad)
+    assert s.nonfinite_count() == 0

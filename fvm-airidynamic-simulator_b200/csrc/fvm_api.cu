@@ -1165,6 +1165,20 @@ int fvm_internal_build_maps(fvm_handle *h) { return build_maps(h); }
 int fvm_internal_compute_dt(fvm_handle *h, const fvm_sim_params *p, float *dt) { return fvm_compute_dt(h, p, dt); }
 int fvm_internal_set_error(int code, const char *msg) { return set_err(code, "%s", msg); }
 
+extern "C" int fvm_debug_wait_timeout(fvm_handle *h, long long limit_cycles) {
+    CHECK_INIT(h);
+    if (limit_cycles <= 0 || limit_cycles > kWaitCycles)
+        return set_err(FVM_ERR_INVALID, "fvm_debug_wait_timeout: limit must be in 1..%lld cycles", kWaitCycles);
+    CK(cudaStreamSynchronize(h->stream));
+    CK(launch_wait_probe(h->sc, limit_cycles, h->stream));
+    const int r = check_device_error(h);
+    // clear the error word the probe set, so the solve goes on
+    unsigned zero = 0;
+    CK(cudaMemcpyAsync(&h->sc->err, &zero, sizeof(unsigned), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return r;
+}
+
 extern "C" int fvm_debug_ghost_table(fvm_handle *h, int *out, int cap, int *count_out) {
     CHECK_INIT(h);
     static_assert(sizeof(GhostInfo) == 6 * sizeof(int), "GhostInfo layout");

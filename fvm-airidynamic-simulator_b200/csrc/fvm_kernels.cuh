@@ -43,6 +43,8 @@ cudaError_t launch_ghost_batch(const BatchInst *insts, const GhostChunk *chunks,
                                cudaStream_t st);
 // Ghost-cell pass over the ghost table.
 cudaError_t launch_ghost(const GhostArgs &a, cudaStream_t st);
+// Bounded wait on an mbarrier nothing arrives on (expires after limit_cycles).
+cudaError_t launch_wait_probe(DevScalars *sc, long long limit_cycles, cudaStream_t st);
 // Phase-1 boundary conditions in place on a whole state (set-up path).
 cudaError_t launch_bc_phase1(const GridDesc &g, float *U, const uint8_t *mask, const Freestream &fs, cudaStream_t st);
 // CFL maxima of a state (speed over all cells; nu = mu(T)/rho, mu = 0 in solids),

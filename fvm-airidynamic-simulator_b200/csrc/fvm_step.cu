@@ -1163,6 +1163,26 @@ cudaError_t launch_ghost_batch(const BatchInst *insts, const GhostChunk *chunks,
     return cudaGetLastError();
 }
 
+// Failure-path probe: one warp waits, through the kernels' own bounded wait,
+// on an mbarrier nothing arrives on, so the wait must give up after `limit`
+// SM cycles and record the timeout in the error word, as a stuck staging
+// load would.
+__global__ void k_wait_probe(DevScalars *sc, long long limit) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    const bool ok = mbar_wait_bounded(&bar, 0u, limit);
+    if (!ok && threadIdx.x == 0) record_error(sc, kErrTimeout);
+}
+
+cudaError_t launch_wait_probe(DevScalars *sc, long long limit_cycles, cudaStream_t st) {
+    k_wait_probe<<<1, 32, 0, st>>>(sc, limit_cycles);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_ghost(const GhostArgs &a, cudaStream_t st) {
     int blocks = (a.n + 127) / 128;
     if (blocks < 1) blocks = 1;

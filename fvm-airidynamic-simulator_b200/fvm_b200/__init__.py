@@ -36,7 +36,8 @@ EXPORTS = [
     "fvm_server_poll", "fvm_server_wait", "fvm_server_drain", "fvm_server_get_stats", "fvm_server_destroy",
     "fvm_state_max_noalloc", "fvm_shedding_stats", "fvm_colormap_to_device", "fvm_colormap_table",
     "fvm_save_checkpoint", "fvm_load_checkpoint", "fvm_checkpoint_info", "fvm_autotune", "fvm_get_tune",
-    "fvm_set_tune", "fvm_nonfinite_count", "fvm_debug_stage1", "fvm_debug_ghost_table", "fvm_build_info",
+    "fvm_set_tune", "fvm_nonfinite_count", "fvm_debug_stage1", "fvm_debug_ghost_table",
+    "fvm_debug_wait_timeout", "fvm_build_info",
 ]
 
 
@@ -139,6 +140,7 @@ def load_library(path=None):
     lib.fvm_get_tune.argtypes = [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i)]
     lib.fvm_set_tune.argtypes = [vp, i, i, i]
     lib.fvm_nonfinite_count.argtypes = [vp, C.POINTER(C.c_ulonglong), i]
+    lib.fvm_debug_wait_timeout.argtypes = [vp, C.c_longlong]
     lib.fvm_debug_ghost_table.argtypes = [vp, vp, i, C.POINTER(i)]
     _lib = lib
     return lib

@@ -425,6 +425,14 @@ int fvm_debug_stage1(fvm_handle *h, float dt, int with_ghost, float *rho, float 
  * `out` (cap entries); *count_out receives the number of ghost cells. */
 int fvm_debug_ghost_table(fvm_handle *h, int *out, int cap, int *count_out);
 
+/* Test hook for the failure path of the kernels' bounded waits: launches one
+ * warp that waits on a barrier nothing completes, so its wait gives up after
+ * limit_cycles SM cycles (1..4e9; two million is about a millisecond) and sets
+ * the timeout bit of this solve's device error word.  Returns the status a
+ * step would then report (FVM_ERR_TIMEOUT), clears the error word and leaves
+ * the solve's state untouched and usable.  No reference counterpart. */
+int fvm_debug_wait_timeout(fvm_handle *h, long long limit_cycles);
+
 /* Library build description (arch, flags). */
 const char *fvm_build_info(void);
 

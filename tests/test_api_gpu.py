@@ -295,3 +295,22 @@ def test_nonfinite_cells_are_counted_on_the_device(name, field):
     bad = int((~np.isfinite(s.fields())).any(axis=0).sum())
     assert n >= 1 and bad >= 1, (n, bad)
     assert s.nonfinite_count() == 0
+
+
+def test_bounded_wait_expires_with_a_status_and_the_solve_goes_on():
+    """The kernels' bounded wait, made to run out on a barrier nothing
+    completes (about a millisecond), sets the device error word; the call
+    reports FVM_ERR_TIMEOUT, and the same solve then steps on bitwise like an
+    undisturbed twin."""
+    s, p, e = _solver()
+    twin, q, _ = _solver()
+    p.dt = q.dt = s.compute_dt()
+    s.step(3)
+    twin.step(3)
+    assert s.lib.fvm_debug_wait_timeout(s.h, 2_000_000) == 5
+    assert b"bounded device wait" in s.lib.fvm_last_error()
+    assert s.lib.fvm_debug_wait_timeout(s.h, 0) == 1
+    s.step(3)
+    twin.step(3)
+    s.synchronize()
+    assert np.array_equal(s.fields().view(np.uint32), twin.fields().view(np.uint32))

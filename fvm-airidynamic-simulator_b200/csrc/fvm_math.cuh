@@ -278,14 +278,20 @@ __device__ __forceinline__ void face_flux(bool valid, bool near_wall, const Prim
 
 // updateKernel body for a non-wall cell (src/solver.cu:1736-1875).
 // fR/fL: x-face fluxes at i+1/2 and i-1/2, fT/fB: y-faces at j+1/2, j-1/2.
-// rho_*: raw densities of the four neighbours and the centre, p_c: primitive p.
+// uR, uL, vT, vB: the faces' velocities for the rho_e source (face_velocity of
+// each face, the same value from either side), p_c: primitive p.
 struct UpdateArgs {
     float dt, inv_dx, inv_dy;
 };
+// Face velocity of the rho_e source term: mass flux over the mean of the two
+// cells' clamped densities (src/solver.cu:1772-1794).
+__device__ __forceinline__ float face_velocity(float mass_flux, float rho_a, float rho_b) {
+    return mass_flux / (0.5f * (fmaxf(rho_a, MIN_DENSITY) + fmaxf(rho_b, MIN_DENSITY)));
+}
 __device__ __forceinline__ void update_cell(const float U[5], const float fR[5], const float fL[5], const float fT[5],
-                                            const float fB[5], float rho_xR, float rho_xL, float rho_yT,
-                                            float rho_yB, float p_c, bool edge_x, bool edge_y, bool interior,
-                                            const UpdateArgs &a, float out[5]) {
+                                            const float fB[5], float uR, float uL, float vT, float vB, float p_c,
+                                            bool edge_x, bool edge_y, bool interior, const UpdateArgs &a,
+                                            float out[5]) {
     float dFx[5], dFy[5];
 #pragma unroll
     for (int k = 0; k < 5; k++) {
@@ -302,16 +308,7 @@ __device__ __forceinline__ void update_cell(const float U[5], const float fR[5],
     }
     float source_rho_e = 0.0f;
     if (interior) {
-        float rho_c = fmaxf(U[0], MIN_DENSITY);
-        float rxR = fmaxf(rho_xR, MIN_DENSITY);
-        float rxL = fmaxf(rho_xL, MIN_DENSITY);
-        float u_face_R = fR[0] / (0.5f * (rho_c + rxR));
-        float u_face_L = fL[0] / (0.5f * (rxL + rho_c));
-        float ryT = fmaxf(rho_yT, MIN_DENSITY);
-        float ryB = fmaxf(rho_yB, MIN_DENSITY);
-        float v_face_T = fT[0] / (0.5f * (rho_c + ryT));
-        float v_face_B = fB[0] / (0.5f * (ryB + rho_c));
-        float div_v = (u_face_R - u_face_L) * a.inv_dx + (v_face_T - v_face_B) * a.inv_dy;
+        float div_v = (uR - uL) * a.inv_dx + (vT - vB) * a.inv_dy;
         source_rho_e = -p_c * div_v;
     }
     const float dt = a.dt;

@@ -120,7 +120,7 @@ struct StageLayout {
     static constexpr size_t p_off = bl_off + bl_bytes;
     static constexpr size_t p_bytes = (size_t)PP * 2 * NT * 16;
     static constexpr size_t x_off = p_off + p_bytes;
-    static constexpr size_t x_bytes = (size_t)XP * 2 * 5 * NT * 4;
+    static constexpr size_t x_bytes = (size_t)XP * 2 * 6 * NT * 4;  // 5 fluxes + face velocity
     static constexpr size_t m_off = x_off + x_bytes;
     static constexpr size_t m_bytes = (size_t)PP * 2 * NT;
     static constexpr size_t bar_off = (m_off + m_bytes + 15) & ~(size_t)15;
@@ -222,6 +222,7 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
     int kr = base % KP, par = (base / KP) & 1, ku = (base + KP - 1) % KP;
     int pc0 = 0, pc1 = 4, pc2 = 2;  // P/M rows of row pairs q, q-1, q-2
     float fyB[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};  // y-face below row r-2
+    float vfB = 0.0f;                                // and its face velocity
     float sy2[4] = {0.0f, 0.0f, 0.0f, 0.0f};         // y-slopes of row r-2
     bool ok_all = true;
 
@@ -230,7 +231,7 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
         const uint32_t nA = __ldg(mcol + (size_t)clampi(r + 2, 0, ny - 1) * g.pitch);
         const uint32_t nB = __ldg(mcol + (size_t)clampi(r + 3, 0, ny - 1) * g.pitch);
         // ---- phase 1: primitives + masks of rows r, r+1
-        const int s0 = pc0 >> 1, s1 = pc1 >> 1, s2 = pc2 >> 1;  // pair slots of q, q-1, q-2
+        const int s0 = pc0 >> 1, s1 = pc1 >> 1;  // pair slots of q, q-1
         bool ok = mbar_wait_bounded(&bars[kr], (uint32_t)par);
         if (ok) {
             float rho[2], u[2], v[2], p[2];
@@ -256,13 +257,9 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
         // column cy, rows r-3 .. r: pairs q-2 (rows r-4, r-3), q-1 (r-2, r-1), q (r, r+1)
         const float4 A1 = PA[s1 * NT + cy], B1 = PB[s1 * NT + cy];
         const float4 A0 = PA[s0 * NT + cy], B0 = PB[s0 * NT + cy];
-        const float rho3 = PA[s2 * NT + cy].y;                       // density of row r-3
         const float4 c2 = make_float4(A1.x, A1.z, B1.x, B1.z);        // row r-2 (rho, u, v, p)
         const float4 c1 = make_float4(A1.y, A1.w, B1.y, B1.w);        // row r-1
         const float rho0 = A0.x;                                      // density of row r
-        // densities of rows r-2, r-1 beside column cy
-        const float2 rhoE = *reinterpret_cast<const float2 *>(&PA[s1 * NT + cy + 1]);
-        const float2 rhoW = *reinterpret_cast<const float2 *>(&PA[s1 * NT + cy - 1]);
         float fy0[5], fy1[5];
         {
             // y-faces (r-2 | r-1) and (r-1 | r) as one lane pair; the y-slopes
@@ -273,6 +270,8 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
             face_pair_y<SCHEME, LIM>((my0 & MB_YV) != 0, (my0 & MB_YN) != 0, (my1 & MB_YV) != 0, (my1 & MB_YN) != 0,
                                      lo, mid, hi, sy2, fy0, fy1);
         }
+        // face velocities of the two y-faces (the face below row r-2 is carried)
+        const float vf0 = face_velocity(fy0[0], c2.x, c1.x), vf1 = face_velocity(fy1[0], c1.x, rho0);
 #pragma unroll
         for (int h = 0; h < 2; h++) {
             const int urow = r - 2 + h;
@@ -286,7 +285,7 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
 #pragma unroll
                     for (int k = 0; k < 5; k++) Un[k] = Uc[k];
                 } else {
-                    const float *Xs = X + h * 5 * NT + t;
+                    const float *Xs = X + h * 6 * NT + t;
                     float fR[5], fL[5], fT[5], fB[5];
 #pragma unroll
                     for (int k = 0; k < 5; k++) {
@@ -296,12 +295,10 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
                         fB[k] = h ? fy0[k] : fyB[k];
                     }
                     const float4 pc = h ? c1 : c2;
-                    const float rxR = h ? rhoE.y : rhoE.x, rxL = h ? rhoW.y : rhoW.x;
-                    const float ryT = h ? rho0 : c1.x;
-                    const float ryB = h ? c2.x : rho3;
+                    const float vT = h ? vf1 : vf0, vB = h ? vf0 : vfB;
                     const bool edge_y = (urow == 0 || urow == ny - 1);
-                    update_cell(Uc, fR, fL, fT, fB, rxR, rxL, ryT, ryB, pc.w, edge_x, edge_y, !edge_x && !edge_y, ua,
-                                Un);
+                    update_cell(Uc, fR, fL, fT, fB, Xs[5 * NT + 1], Xs[5 * NT], vT, vB, pc.w, edge_x, edge_y,
+                                !edge_x && !edge_y, ua, Un);
                 }
                 if (STAGE == 2) {
                     const float *b = bl + (size_t)(ku * 2 + h) * L::BSLOT + t;
@@ -323,6 +320,7 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
         }
 #pragma unroll
         for (int k = 0; k < 5; k++) fyB[k] = fy1[k];
+        vfB = vf1;
         fence_proxy_async_smem();
         __syncthreads();
         // the input slot of pair q-1 is free now: stage pair q-1+KP into it
@@ -343,8 +341,11 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
 #pragma unroll
                 for (int k = 0; k < 5; k++) {
                     Xs[k * NT] = fx0[k];
-                    Xs[(5 + k) * NT] = fx1[k];
+                    Xs[(6 + k) * NT] = fx1[k];
                 }
+                // face velocities for the rho_e source of both adjacent cells
+                Xs[5 * NT] = face_velocity(fx0[0], A[tx + 1].x, A[tx + 2].x);
+                Xs[11 * NT] = face_velocity(fx1[0], A[tx + 1].y, A[tx + 2].y);
             }
         }
         pc2 = pc1;

@@ -459,6 +459,14 @@ extern "C" int fvm_batch_read_fields(fvm_batch *b, int id, float *rho, float *rh
     return FVM_OK;
 }
 
+extern "C" int fvm_batch_nonfinite_count(fvm_batch *b, int id, unsigned long long *count) {
+    CHECK_BATCH(b);
+    fvm_handle *h = inst_of(b, id);
+    if (!h || !count) return berr(FVM_ERR_INVALID, "unknown instance id or null output");
+    BCK(cudaStreamSynchronize(b->stream));
+    return fvm_nonfinite_count(h, count, 0);
+}
+
 extern "C" int fvm_batch_diagnostics(fvm_batch *b, int id, fvm_diag *out) {
     CHECK_BATCH(b);
     fvm_handle *h = inst_of(b, id);

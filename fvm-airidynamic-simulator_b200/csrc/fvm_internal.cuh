@@ -42,8 +42,8 @@ struct DevScalars {
     float dt;         // dt the next step uses (read by the step kernels)
     float t;          // simulated time (advanced on the device under recompute)
     unsigned counter; // last-block counter of the ghost pass
-    unsigned err;     // error word (kErrTimeout, kErrNonFinite)
-    unsigned nonfinite;
+    unsigned err;        // error word (kErrTimeout, kErrSmemAlign)
+    unsigned nonfinite;  // (cell, step) pairs with a non-finite new state
     float dt_last;    // dt of the last completed step (recompute policy)
     unsigned parity;  // batched solves: which ping-pong buffer holds U^n
     unsigned pad;

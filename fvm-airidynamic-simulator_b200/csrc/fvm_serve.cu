@@ -150,7 +150,10 @@ static fvm_result retire(fvm_server *s, const Request &r, int status) {
         x.t_final = q.t_current;
         x.dt_last = q.dt;
     }
-    if (rc == FVM_OK && !(std::isfinite(x.diag.mass) && std::isfinite(x.diag.energy) && std::isfinite(x.diag.cd)))
+    unsigned long long nonfinite = 0;
+    if (rc == FVM_OK) rc = fvm_batch_nonfinite_count(s->b, r.id, &nonfinite);
+    if (rc == FVM_OK && (nonfinite > 0 || !(std::isfinite(x.diag.mass) && std::isfinite(x.diag.energy) &&
+                                            std::isfinite(x.diag.cd))))
         rc = FVM_ERR_NONFINITE;
     fvm_batch_retire(s->b, r.id);
     x.status = rc;

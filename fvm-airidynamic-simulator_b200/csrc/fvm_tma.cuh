@@ -12,7 +12,6 @@ namespace fvm {
 
 constexpr long long kWaitCycles = 4000000000LL;  // ~2 s of SM clock per bounded wait
 constexpr uint32_t kErrTimeout = 1u;       // device error word bits
-constexpr uint32_t kErrNonFinite = 2u;
 constexpr uint32_t kErrSmemAlign = 4u;     // staging area not 128-byte aligned (kernel did nothing)
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {

@@ -31,7 +31,8 @@ EXPORTS = [
     "fvm_diagnostics", "fvm_shock_standoff", "fvm_set_kernel_timing", "fvm_kernel_times",
     "fvm_launch_count", "fvm_batch_create", "fvm_batch_destroy", "fvm_batch_set_stream", "fvm_batch_add",
     "fvm_batch_remove", "fvm_batch_count", "fvm_batch_step", "fvm_batch_synchronize", "fvm_batch_instance",
-    "fvm_batch_read_fields", "fvm_batch_diagnostics", "fvm_batch_memory_usage", "fvm_batch_launch_count",
+    "fvm_batch_read_fields", "fvm_batch_diagnostics", "fvm_batch_nonfinite_count", "fvm_batch_memory_usage",
+    "fvm_batch_launch_count",
     "fvm_batch_instance_bytes", "fvm_batch_retire", "fvm_batch_trim", "fvm_server_create", "fvm_server_submit",
     "fvm_server_poll", "fvm_server_wait", "fvm_server_drain", "fvm_server_get_stats", "fvm_server_destroy",
     "fvm_state_max_noalloc", "fvm_shedding_stats", "fvm_colormap_to_device", "fvm_colormap_table",
@@ -121,6 +122,7 @@ def load_library(path=None):
     lib.fvm_batch_instance.argtypes = [vp, i, Pp]
     lib.fvm_batch_read_fields.argtypes = [vp, i] + [vp] * 5
     lib.fvm_batch_diagnostics.argtypes = [vp, i, C.POINTER(Diag)]
+    lib.fvm_batch_nonfinite_count.argtypes = [vp, i, C.POINTER(C.c_ulonglong)]
     lib.fvm_batch_memory_usage.argtypes = [vp, C.POINTER(sz)]
     lib.fvm_batch_launch_count.argtypes = [vp, C.POINTER(C.c_longlong)]
     lib.fvm_batch_instance_bytes.argtypes = [i, i]
@@ -443,6 +445,12 @@ class Batch:
         d = Diag()
         _check(self.lib.fvm_batch_diagnostics(self.h, int(id_), C.byref(d)))
         return d
+
+    def nonfinite_count(self, id_):
+        """Non-finite (cell, step) count of one instance (fvm_batch_nonfinite_count)."""
+        v = C.c_ulonglong()
+        _check(self.lib.fvm_batch_nonfinite_count(self.h, int(id_), C.byref(v)))
+        return v.value
 
     def memory_usage(self):
         v = C.c_size_t()

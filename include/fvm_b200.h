@@ -275,6 +275,9 @@ int fvm_batch_synchronize(fvm_batch *b);
 int fvm_batch_instance(fvm_batch *b, int id, fvm_sim_params *p_out);
 int fvm_batch_read_fields(fvm_batch *b, int id, float *rho, float *rho_u, float *rho_v, float *E, float *rho_e);
 int fvm_batch_diagnostics(fvm_batch *b, int id, fvm_diag *out);
+/* The instance's non-finite (cell, step) count (fvm_nonfinite_count) since it
+ * was added or reset for its current solve.  No reference counterpart. */
+int fvm_batch_nonfinite_count(fvm_batch *b, int id, unsigned long long *count);
 int fvm_batch_memory_usage(fvm_batch *b, size_t *bytes);
 int fvm_batch_launch_count(fvm_batch *b, long long *count_out);
 /* Device bytes one instance of nx*ny holds (admission estimate). */
@@ -300,7 +303,9 @@ int fvm_batch_trim(fvm_batch *b, size_t keep_bytes, size_t *parked_bytes_out);
 typedef struct fvm_server fvm_server;
 typedef struct {
     long long ticket;
-    int status;        /* FVM_OK, FVM_ERR_BUDGET, FVM_ERR_NONFINITE or the error that ended it */
+    int status;        /* FVM_OK, FVM_ERR_BUDGET, FVM_ERR_NONFINITE (a step produced a NaN or
+                          infinite cell, or the final diagnostics are not finite) or the
+                          error that ended it */
     int steps;         /* steps taken */
     int nx, ny;
     float t_final;     /* simulated time after the last step */

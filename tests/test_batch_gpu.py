@@ -45,6 +45,7 @@ def test_batched_instances_equal_solo_runs_bitwise():
         assert np.array_equal(U.view(np.uint32), B.view(np.uint32)), i
         q = b.instance(i)
         assert q.step == 25 and q.t_current == ps.t_current and q.dt == ps.dt
+        assert b.nonfinite_count(i) == 0
 
 
 def test_batch_add_remove_mid_run():

@@ -606,7 +606,8 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
                 const float4 N = P[(h ? pc0 : pc1 + 1) * NT + tp];
                 const float4 S = h ? P[pc1 * NT + tp] : S0;
                 float rhs[4];
-                viscous_rhs(tC, tE, tW, tNn, tSs, E.x, Wc.x, N.x, S.x, E.y, Wc.y, N.y, S.y, va, rhs);
+                viscous_rhs_xy(tC, tE, tW, tNn, tSs, mk2(E.x, E.y), mk2(Wc.x, Wc.y), mk2(N.x, N.y), mk2(S.x, S.y), va,
+                               rhs);
                 const bool upd = ctype[h] == CT_FLUID && interior_x && urow > 0 && urow < ny - 1;
                 U[h][0] = Uprev[h][0];
 #pragma unroll
@@ -665,8 +666,9 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
     return true;
 }
 
+// 5 CTAs of 128 threads per SM (92 registers, no spills).
 template <int NT, int K>
-__global__ void __launch_bounds__(NT) k_viscous(const __grid_constant__ CUtensorMap tm_in, const StepArgs a) {
+__global__ void __launch_bounds__(NT, 640 / NT) k_viscous(const __grid_constant__ CUtensorMap tm_in, const StepArgs a) {
     using L = ViscLayout<NT, K>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned char *smem = aligned_smem(smem_raw);

@@ -1,8 +1,8 @@
 // fvm_tma.cuh -- TMA tensor loads and mbarrier helpers (sm_100a inline PTX).
 //
 // Loads are local-GPU only and never use cluster multicast.  Every wait on an
-// mbarrier is bounded: after kSpinLimit polls the caller gets `false`, records
-// an error word and leaves the kernel at a uniform point.
+// mbarrier is bounded: after kWaitCycles SM cycles the caller gets `false`,
+// records an error word and leaves the kernel at a uniform point.
 #pragma once
 #include <cstdint>
 #include <cuda.h>

@@ -109,7 +109,7 @@ struct StageLayout {
     static constexpr int NB = (NT + 4 + kBox - 1) / kBox;  // TMA boxes per row
     static constexpr int BW = NB * kBox;  // staged columns [i0-4, i0-4+BW)
     static constexpr int KP = K / 2;   // input ring: K rows staged as K/2 row pairs
-    static constexpr int PP = 3;       // primitive / mask ring (row pairs)
+    static constexpr int PP = 2;       // primitive / mask ring (row pairs)
     static constexpr int XP = 1;       // x-face ring (row pairs)
     static constexpr int SLOT = NB * kBoxStride;                       // floats per staged input row
     static constexpr int BSLOT = (int)(align128((size_t)5 * W * 4) / 4);  // floats per staged blend row
@@ -155,8 +155,8 @@ struct RingPos {
 // The thread that computes a column's y-faces also updates that column, so
 // y-fluxes stay in registers (the face below row r-2 is carried from the
 // previous step).  After the second barrier nothing reads the previous row
-// pair's input slot or the primitives of pair q-2 again, which keeps the
-// rings at K/2 input pairs, 3 primitive pairs and 1 x-face pair.  Returns
+// pair's input slot or primitives again, which keeps the rings at K/2 input
+// pairs, 2 primitive pairs and 1 x-face pair.  Returns
 // false when a bounded wait expired (error recorded; caller must stop).
 template <int NT, int K, int STAGE, int SCHEME, int LIM>
 __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUtensorMap *tm_blend, const StepArgs &a,
@@ -164,7 +164,7 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
                                            unsigned &nbad) {
     using L = StageLayout<NT, K, STAGE>;
     constexpr int W = L::W, KP = L::KP;
-    static_assert(L::PP == 3 && L::XP == 1 && KP >= 2, "ring sizes");
+    static_assert(L::PP == 2 && L::XP == 1 && KP >= 2, "ring sizes");
     float *raw = reinterpret_cast<float *>(smem + L::raw_off);
     float *bl = reinterpret_cast<float *>(smem + L::bl_off);
     // primitives of a row pair, interleaved: PA = {rho_r, rho_r+1, u_r, u_r+1},
@@ -220,7 +220,7 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
     float *outp = a.out + iu;
 
     int kr = base % KP, par = (base / KP) & 1, ku = (base + KP - 1) % KP;
-    int pc0 = 0, pc1 = 4, pc2 = 2;  // P/M rows of row pairs q, q-1, q-2
+    int pc0 = 0, pc1 = 2;  // P/M rows of row pairs q, q-1
     float fyB[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};  // y-face below row r-2
     float vfB = 0.0f;                                // and its face velocity
     float sy2[4] = {0.0f, 0.0f, 0.0f, 0.0f};         // y-slopes of row r-2
@@ -348,9 +348,8 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
                 Xs[11 * NT] = face_velocity(fx1[0], A[tx + 1].y, A[tx + 2].y);
             }
         }
-        pc2 = pc1;
         pc1 = pc0;
-        pc0 = (pc0 == 4) ? 0 : pc0 + 2;
+        pc0 = 2 - pc0;
         kr = ring_next<KP>(kr);
         par ^= (kr == 0) ? 1 : 0;
         ku = ring_next<KP>(ku);
@@ -368,10 +367,10 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
     return true;
 }
 
-// Occupancy targets: 6 CTAs of 128 threads per SM for stage 1 (80 registers,
-// no spills), 5 for stage 2, whose blend ring leaves shared memory for 5.
+// Occupancy target: 6 CTAs of 128 threads per SM (80 registers, no spills;
+// stage 2 with its blend ring takes ~36 KB of shared memory per CTA).
 template <int NT, int K, int STAGE, int SCHEME, int LIM>
-__global__ void __launch_bounds__(NT, (STAGE == 1 ? 768 : 640) / NT)
+__global__ void __launch_bounds__(NT, 768 / NT)
     k_stage(const __grid_constant__ CUtensorMap tm_in, const __grid_constant__ CUtensorMap tm_blend,
             const StepArgs a) {
     using L = StageLayout<NT, K, STAGE>;

@@ -55,8 +55,8 @@ STEP_BYTES_FUSED = 102  # compulsory bytes per cell-update of a fused 5-field RK
 # DRAM bytes (read + write) per launch measured by ncu on the 4096x2048 case
 # and scaled by the cell count to 8192x4096 (profiles/marching_kernels_*.md).
 MEASURED_TRAFFIC = {
-    ("ns_hypersonic_cone", 8192, 4096): {"stage1": 1250167808, "stage2": 1972295680,
-                                         "viscous_pre": 1238436864, "viscous_post": 1240415232},
+    ("ns_hypersonic_cone", 8192, 4096): {"stage1": 1255984128, "stage2": 1973966848,
+                                         "viscous_pre": 1235775488, "viscous_post": 1231261696},
 }
 
 

@@ -617,35 +617,6 @@ __device__ __forceinline__ void stress_heat(float uC, float vC, float TC, float 
                    j_hi, va, out);
 }
 
-// Divergence + forward Euler of the viscous half step for an interior fluid
-// cell (src/solver.cu:2437-2510).  t*: {txx,tyy,txy,qx,qy} at C/E/W/N/S.
-__device__ __forceinline__ void viscous_rhs(const float tC[5], const float tE[5], const float tW[5],
-                                            const float tN[5], const float tS[5], float uE, float uW, float uN,
-                                            float uS, float vE, float vW, float vN, float vS, const ViscArgs &va,
-                                            float rhs[4]) {
-    float dtau_xx_dx = (tE[0] - tW[0]) * va.inv_2dx;
-    float dtau_xy_dy = (tN[2] - tS[2]) * va.inv_2dy;
-    float dtau_xy_dx = (tE[2] - tW[2]) * va.inv_2dx;
-    float dtau_yy_dy = (tN[1] - tS[1]) * va.inv_2dy;
-    float dqx_dx = (tE[3] - tW[3]) * va.inv_2dx;
-    float dqy_dy = (tN[4] - tS[4]) * va.inv_2dy;
-    float du_dx = (uE - uW) * va.inv_2dx;
-    float du_dy = (uN - uS) * va.inv_2dy;
-    float dv_dx = (vE - vW) * va.inv_2dx;
-    float dv_dy = (vN - vS) * va.inv_2dy;
-    float Phi = tC[0] * du_dx + tC[1] * dv_dy + tC[2] * (du_dy + dv_dx);
-    float work_x_ip1 = uE * tE[0] + vE * tE[2];
-    float work_x_im1 = uW * tW[0] + vW * tW[2];
-    float work_y_jp1 = uN * tN[2] + vN * tN[1];
-    float work_y_jm1 = uS * tS[2] + vS * tS[1];
-    float dwork_dx = (work_x_ip1 - work_x_im1) * va.inv_2dx;
-    float dwork_dy = (work_y_jp1 - work_y_jm1) * va.inv_2dy;
-    rhs[0] = dtau_xx_dx + dtau_xy_dy;
-    rhs[1] = dtau_xy_dx + dtau_yy_dy;
-    rhs[2] = -dqx_dx - dqy_dy + dwork_dx + dwork_dy;
-    rhs[3] = -dqx_dx - dqy_dy + Phi;
-}
-
 // CFL quantities (src/solver.cu:2729-2739, :2679-2687)
 __device__ __forceinline__ float wave_speed(float u, float v, float p, float rho_raw) {
     float c = sqrtf(GAMMA * p / (rho_raw + 1e-10f));

@@ -219,9 +219,11 @@ __device__ __forceinline__ void face_pair_y(bool valid0, bool near0, bool valid1
     sy_lo[3] = sm.p.y;
 }
 
-// Divergence terms of the viscous half step for one interior fluid cell, as
-// viscous_rhs (fvm_math.cuh; src/solver.cu:2437-2510), with the x and y
-// parts of each derivative pair in one FP32x2 lane pair: (du/dx, dv/dx),
+// Divergence terms of the viscous half step for one interior fluid cell
+// (src/solver.cu:2437-2510): rhs = {d(tau_xx)/dx + d(tau_xy)/dy,
+// d(tau_xy)/dx + d(tau_yy)/dy, -div q + div(tau . v), -div q + Phi}, central
+// differences, with the x and y parts of each derivative pair in one FP32x2
+// lane pair: (du/dx, dv/dx),
 // (du/dy, dv/dy), (dtau_xx/dx, dtau_xy/dx), (dtau_xy/dy, dtau_yy/dy),
 // (dqx/dx, dqy/dy), (dwork/dx, dwork/dy).  vE..vS are the neighbours'
 // (u, v), already a register pair in the primitive ring's {u, v, T, mu}

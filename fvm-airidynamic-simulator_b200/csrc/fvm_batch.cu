@@ -286,17 +286,25 @@ extern "C" int fvm_batch_add(fvm_batch *b, const fvm_sim_params *p, int *id_out)
             return r;
         }
     }
-    // device scalars of the fresh solve
+    // device scalars of the fresh solve; on a CUDA error the instance is
+    // destroyed here, so its memory never stays outside the batch's accounting
+    auto fail = [&](cudaError_t e) {
+        fvm_destroy(h);
+        return berr(FVM_ERR_CUDA, cudaGetErrorString(e));
+    };
     DevScalars init;
-    BCK(cudaMemcpyAsync(&init, h->sc, sizeof init, cudaMemcpyDeviceToHost, b->admit));
-    BCK(cudaStreamSynchronize(b->admit));
+    cudaError_t ce;
+    if ((ce = cudaMemcpyAsync(&init, h->sc, sizeof init, cudaMemcpyDeviceToHost, b->admit)) != cudaSuccess ||
+        (ce = cudaStreamSynchronize(b->admit)) != cudaSuccess)
+        return fail(ce);
     init.dt = dt;
     init.t = p->t_current;
     init.parity = 0;
     init.counter = 0;
     init.red[0] = init.red[1] = 0.0f;
-    BCK(cudaMemcpyAsync(h->sc, &init, sizeof init, cudaMemcpyHostToDevice, b->admit));
-    BCK(cudaStreamSynchronize(b->admit));
+    if ((ce = cudaMemcpyAsync(h->sc, &init, sizeof init, cudaMemcpyHostToDevice, b->admit)) != cudaSuccess ||
+        (ce = cudaStreamSynchronize(b->admit)) != cudaSuccess)
+        return fail(ce);
     h->stream = b->stream;
     int id = -1;
     for (size_t k = 0; k < b->slots.size(); k++)

@@ -12,11 +12,13 @@
 //
 // How: the same per-cell quantity as k_max_reduce (fvm_aux.cu), one CTA per
 // grid row.  Each CTA writes its row maximum into a fixed file-scope device
-// array; the last CTA to arrive reduces the row maxima, stores the result in
-// the same array and re-arms the arrival counter.  The array's size caps the
-// number of rows; larger grids are rejected before anything is launched.
-#include <atomic>
+// array; the last CTA to arrive reduces the row maxima and stores the result
+// in the same array.  The array's size caps the number of rows; larger grids
+// are rejected before anything is launched.
+#include <cuda.h>
+
 #include <cstdio>
+#include <mutex>
 
 #include "fvm_handle.h"
 #include "fvm_tma.cuh"
@@ -35,9 +37,12 @@ constexpr int kThreads = 256;
 
 // Word layout: [0, kNoAllocMaxRows) row maxima (float bits), kResultWord the
 // result, kArrivalWord the arrival counter.  Only the arrival counter must be
-// zero when a launch starts: the module loads it zeroed and the last CTA of
-// every launch sets it back to zero.  Row maxima are written before they are
-// read in each launch, so they need no initial value.
+// zero when a launch starts.  The host clears it with a 4-byte memset on the
+// call's stream before every launch, so a launch that never finished (its
+// context torn down mid-flight, say) cannot leave a count behind that would
+// make a later launch pick the wrong last CTA.  The last CTA also sets it back
+// to zero.  Row maxima are written before they are read in each launch, so
+// they need no initial value.
 static __device__ __align__(256) unsigned int g_noalloc_scratch[kScratchWords];
 
 // what = 0: temperature, what = 1: local Mach number, cell by cell as
@@ -95,8 +100,31 @@ __global__ void __launch_bounds__(kThreads)
 
 using namespace fvm;
 
-// Device address of g_noalloc_scratch, looked up once per device.
-static std::atomic<unsigned int *> g_scratch_addr[kMaxDevices];
+// Device address of g_noalloc_scratch.  The address belongs to one CUDA
+// context's copy of this module, not to a device index: after
+// cudaDeviceReset, or with another context made current on the same device,
+// the old address is stale.  So the cache is keyed on the current context's
+// unique id (cuCtxGetId; ids are never reused within a process), and the
+// lookup is repeated whenever the id changes.
+namespace {
+typedef CUresult (*PFN_ctxGetCurrent_t)(CUcontext *);
+typedef CUresult (*PFN_ctxGetId_t)(CUcontext, unsigned long long *);
+struct ScratchSlot {
+    unsigned long long ctx_id = 0;
+    unsigned int *addr = nullptr;
+};
+std::mutex g_scratch_mu;
+ScratchSlot g_scratch_slot[kMaxDevices];
+
+template <class F>
+F driver_fn(const char *name) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint(name, &p, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess)
+        return nullptr;
+    return reinterpret_cast<F>(p);
+}
+}  // namespace
 
 static int noalloc_err(int code, const char *fmt, long long a, long long b) {
     char buf[256];
@@ -127,13 +155,47 @@ extern "C" int fvm_state_max_noalloc(const float *state, int nx, int ny, size_t 
     if (dev < 0 || dev >= kMaxDevices)
         return noalloc_err(FVM_ERR_UNSUPPORTED, "fvm_state_max_noalloc: device %lld beyond the %lld supported", dev,
                            kMaxDevices);
-    unsigned int *scratch = g_scratch_addr[dev].load(std::memory_order_acquire);
-    if (!scratch) {
-        e = cudaGetSymbolAddress((void **)&scratch, g_noalloc_scratch);
-        if (e != cudaSuccess) return fvm_internal_set_error(FVM_ERR_CUDA, cudaGetErrorString(e));
-        g_scratch_addr[dev].store(scratch, std::memory_order_release);
-    }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // the call ends with a copy into pageable host memory and a stream
+    // synchronize, neither of which a capturing stream allows
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if ((e = cudaStreamIsCapturing(st, &cap)) != cudaSuccess)
+        return fvm_internal_set_error(FVM_ERR_CUDA, cudaGetErrorString(e));
+    if (cap != cudaStreamCaptureStatusNone)
+        return fvm_internal_set_error(FVM_ERR_STATE, "fvm_state_max_noalloc: the stream is being captured");
+    static const PFN_ctxGetCurrent_t ctx_current = driver_fn<PFN_ctxGetCurrent_t>("cuCtxGetCurrent");
+    static const PFN_ctxGetId_t ctx_id_of = driver_fn<PFN_ctxGetId_t>("cuCtxGetId");
+    if (!ctx_current || !ctx_id_of)
+        return fvm_internal_set_error(FVM_ERR_UNSUPPORTED, "fvm_state_max_noalloc: cuCtxGetId unavailable");
+    CUcontext ctx = nullptr;
+    if (ctx_current(&ctx) != CUDA_SUCCESS)
+        return fvm_internal_set_error(FVM_ERR_CUDA, "fvm_state_max_noalloc: cuCtxGetCurrent failed");
+    if (!ctx) {
+        // no context current on this thread yet: the runtime's symbol lookup
+        // makes the device's primary context current (allocating nothing)
+        unsigned int *probe = nullptr;
+        if ((e = cudaGetSymbolAddress((void **)&probe, g_noalloc_scratch)) != cudaSuccess)
+            return fvm_internal_set_error(FVM_ERR_CUDA, cudaGetErrorString(e));
+        if (ctx_current(&ctx) != CUDA_SUCCESS || !ctx)
+            return fvm_internal_set_error(FVM_ERR_CUDA, "fvm_state_max_noalloc: no current CUDA context");
+    }
+    unsigned long long ctx_id = 0;
+    if (ctx_id_of(ctx, &ctx_id) != CUDA_SUCCESS)
+        return fvm_internal_set_error(FVM_ERR_CUDA, "fvm_state_max_noalloc: cuCtxGetId failed");
+    unsigned int *scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_scratch_mu);
+        ScratchSlot &slot = g_scratch_slot[dev];
+        if (slot.addr == nullptr || slot.ctx_id != ctx_id) {
+            e = cudaGetSymbolAddress((void **)&scratch, g_noalloc_scratch);
+            if (e != cudaSuccess) return fvm_internal_set_error(FVM_ERR_CUDA, cudaGetErrorString(e));
+            slot.addr = scratch;
+            slot.ctx_id = ctx_id;
+        }
+        scratch = slot.addr;
+    }
+    if ((e = cudaMemsetAsync(scratch + kArrivalWord, 0, sizeof(unsigned int), st)) != cudaSuccess)
+        return fvm_internal_set_error(FVM_ERR_CUDA, cudaGetErrorString(e));
     k_state_max_rows<<<ny, kThreads, 0, st>>>(what, nx, pitch, plane, state, scratch);
     if ((e = cudaGetLastError()) != cudaSuccess) return fvm_internal_set_error(FVM_ERR_CUDA, cudaGetErrorString(e));
     e = cudaMemcpyAsync(out, scratch + kResultWord, sizeof(float), cudaMemcpyDeviceToHost, st);

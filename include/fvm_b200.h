@@ -137,7 +137,11 @@ int fvm_set_ext(fvm_handle *h, const fvm_ext *ext);
 /* -------------------------------------------------------------- stepping */
 /* CFDSolver::step (src/solver.cu:3289-3412): one SSP-RK2 step (Strang split
  * when p->enable_viscosity); advances p->t_current and p->step.  Under
- * FVM_DT_RECOMPUTE, p->dt receives the dt that was used. */
+ * FVM_DT_RECOMPUTE, p->dt receives the dt that was used, and the call waits
+ * for the step and reports a device error word (FVM_ERR_TIMEOUT after an
+ * expired bounded wait) itself.  Under FVM_DT_FIXED the call returns once the
+ * work is queued; a device error of those steps is reported by the next
+ * fvm_synchronize (or the next call that reads device scalars). */
 int fvm_step(fvm_handle *h, fvm_sim_params *p);
 /* n steps back to back (graph-captured after the first call for a given shape). */
 int fvm_steps(fvm_handle *h, fvm_sim_params *p, int n);
@@ -355,10 +359,14 @@ int fvm_server_destroy(fvm_server *s);
  * point of the call (memory committed up front to solve instances, no handle
  * to create): the reduction scratch is a fixed array inside the library,
  * enough for ny <= 16384 rows; a larger ny is rejected with FVM_ERR_INVALID
- * before anything runs.  The first call on each device looks up that array's
- * address (cudaGetSymbolAddress, which may load the library's device code):
- * make that first call before any stream capture begins.  All calls on one
- * device share the array, so calls must not overlap: do not call it from two
+ * before anything runs.  The array's device address is looked up
+ * (cudaGetSymbolAddress) on the first call in each CUDA context and again
+ * whenever the current context changes (after cudaDeviceReset, say).  Every
+ * call clears the array's arrival counter, launches one kernel, copies the
+ * result to *out and synchronizes `stream`, so it cannot run on a stream that
+ * is being captured: it then returns FVM_ERR_STATE and does nothing.  All
+ * calls on one device share the array and it keeps the last call's
+ * contents, so calls must not overlap on the GPU: do not call it from two
  * host threads at once for the same device. */
 int fvm_state_max_noalloc(const float *state, int nx, int ny, size_t pitch, size_t plane, int what, float *out,
                           void *stream);

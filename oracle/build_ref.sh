@@ -4,15 +4,17 @@
 # (--use_fast_math -O3, CMakeLists.txt:277-298) retargeted to sm_100a:
 #   oracle/_ref/libfvm_ref.so      src/solver.cu + oracle/ref_harness.cu
 #   oracle/_ref/kernel_benchmark   src/solver.cu + src/test/kernel_benchmark.cu
-# Test infrastructure only.  Needs the reference checkout at $FVM_REFERENCE
-# (default /root/reference); without it the script does nothing.
+# Test infrastructure only.  The reference checkout is $FVM_REFERENCE when
+# set, else a directory named `reference` beside this repository; when
+# neither holds the reference sources the script says so and does nothing
+# (machines that only run the prebuilt files need no sources).
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
-REF="${FVM_REFERENCE:-/root/reference}"
+REF="${FVM_REFERENCE:-$(cd "$HERE/../.." && pwd)/reference}"
 OUT="$HERE/_ref"
 NVCC="${NVCC:-/usr/local/cuda/bin/nvcc}"
 if [ ! -f "$REF/src/solver.cu" ]; then
-    echo "build_ref: no reference sources at $REF, skipping"
+    echo "build_ref: no reference sources at $REF (set FVM_REFERENCE to the checkout), skipping"
     exit 0
 fi
 mkdir -p "$OUT"

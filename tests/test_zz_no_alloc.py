@@ -73,3 +73,29 @@ def test_noalloc_max_at_the_row_limit():
         rc, T = _call(lib, U.data_ptr(), nx, ny, nx, nx * ny, 0)
         assert rc == 0, lib.fvm_last_error()
         assert abs(T - 700.0) <= 1e-3, T
+
+
+@pytest.mark.gpu
+def test_noalloc_refuses_a_capturing_stream_and_works_after():
+    import torch
+    lib = fvm_b200.load_library()
+    nx, ny = 64, 32
+    U = torch.ones((5, ny, nx), dtype=torch.float32, device="cuda")
+    U[3] *= 2.5e5
+    U[4] *= 2.5e5
+    torch.cuda.synchronize()
+    st = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    x = torch.zeros(4, device="cuda")
+    with torch.cuda.graph(g, stream=st):
+        x.add_(1.0)
+        out = C.c_float(-1.0)
+        rc = lib.fvm_state_max_noalloc(C.c_void_p(U.data_ptr()), nx, ny, nx, nx * ny, 0, C.byref(out),
+                                       C.c_void_p(st.cuda_stream))
+    assert rc == 4 and b"captured" in lib.fvm_last_error()  # FVM_ERR_STATE, nothing queued
+    g.replay()
+    torch.cuda.synchronize()
+    assert float(x[0]) == 1.0
+    rc, T = _call(lib, U.data_ptr(), nx, ny, nx, nx * ny, 0)
+    assert rc == 0, lib.fvm_last_error()
+    assert abs(T - 2.5e5 * 0.4 / 287.05) <= 1e-3 * T, T

@@ -363,12 +363,7 @@ cudaError_t launch_diagnostics(const GridDesc &g, const float *U, const uint8_t 
     d.g = g;
     d.U = U;
     d.mask = mask;
-    d.va.inv_2dx = 0.5f / g.dx;
-    d.va.inv_2dy = 0.5f / g.dy;
-    d.va.inv_dx = 1.0f / g.dx;
-    d.va.inv_dy = 1.0f / g.dy;
-    d.va.prandtl = prandtl;
-    d.va.ref_prandtl = ref_prandtl != 0;
+    d.va = viscous_args(g.dx, g.dy, prandtl, ref_prandtl != 0);
     k_diag_partial<<<nparts, 256, 0, st>>>(d, viscous, partials);
     k_diag_final<<<1, 32, 0, st>>>(partials, nparts, out8);
     return cudaGetLastError();

@@ -53,19 +53,34 @@ struct Prim {  // flux-stencil state: raw conserved density + primitive velocity
     float rho, u, v, p;
 };
 
+// Approximate reciprocal (the same hardware approximation the fast-math
+// division a / b multiplies by); one reciprocal serves every quotient with
+// the same divisor.
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// The dual-energy switch eta = rho_e / E < 1e-3 of the reference (eta = 1
+// when E <= 0), evaluated as rho_e < 1e-3 * E for E > 0 (no division).
+__device__ __forceinline__ bool dual_energy_low(float rho_e, float E) {
+    return E > 0.0f && rho_e < ETA_THRESHOLD * E;
+}
+
 // computePrimitivesKernelInline (src/solver.cu:862-894)
 __device__ __forceinline__ void prim_from_cons(float rho, float rho_u, float rho_v, float E, float rho_e,
                                                float &u, float &v, float &p, float &T) {
     float rho_val = fmaxf(rho, MIN_DENSITY);
-    float u_val = rho_u / rho_val;
-    float v_val = rho_v / rho_val;
+    const float inv_rho = rcp_approx(rho_val);
+    float u_val = rho_u * inv_rho;
+    float v_val = rho_v * inv_rho;
     float ke = 0.5f * rho_val * (u_val * u_val + v_val * v_val);
     float e_from_E = E - ke;
-    float eta = (E > 0.0f) ? (rho_e / E) : 1.0f;
-    float e_internal = (eta < ETA_THRESHOLD) ? rho_e : e_from_E;
+    float e_internal = dual_energy_low(rho_e, E) ? rho_e : e_from_E;
     float p_val = (GAMMA - 1.0f) * e_internal;
     p_val = fmaxf(p_val, MIN_PRESSURE);
-    float T_val = p_val / (rho_val * R_GAS);
+    float T_val = p_val * inv_rho * (1.0f / R_GAS);
     T_val = fminf(T_val, MAX_TEMPERATURE);
     T_val = fmaxf(T_val, MIN_TEMPERATURE);
     u = u_val;
@@ -286,60 +301,51 @@ struct UpdateArgs {
 // Face velocity of the rho_e source term: mass flux over the mean of the two
 // cells' clamped densities (src/solver.cu:1772-1794).
 __device__ __forceinline__ float face_velocity(float mass_flux, float rho_a, float rho_b) {
-    return mass_flux / (0.5f * (fmaxf(rho_a, MIN_DENSITY) + fmaxf(rho_b, MIN_DENSITY)));
+    return mass_flux * rcp_approx(0.5f * (fmaxf(rho_a, MIN_DENSITY) + fmaxf(rho_b, MIN_DENSITY)));
 }
 __device__ __forceinline__ void update_cell(const float U[5], const float fR[5], const float fL[5], const float fT[5],
                                             const float fB[5], float uR, float uL, float vT, float vB, float p_c,
                                             bool edge_x, bool edge_y, bool interior, const UpdateArgs &a,
                                             float out[5]) {
-    float dFx[5], dFy[5];
+    // U - dt (dF/dx + dF/dy) as U - (dt/dx) dFx - (dt/dy) dFy; the reference
+    // zeroes the flux difference across a domain edge (i = 0 or nx-1 for x,
+    // j = 0 or ny-1 for y), done here by zeroing the coefficient
+    const float dt = a.dt;
+    const float cx = edge_x ? 0.0f : dt * a.inv_dx;
+    const float cy = edge_y ? 0.0f : dt * a.inv_dy;
+    float n[5];
 #pragma unroll
-    for (int k = 0; k < 5; k++) {
-        dFx[k] = (fR[k] - fL[k]) * a.inv_dx;
-        dFy[k] = (fT[k] - fB[k]) * a.inv_dy;
-    }
-    if (edge_x) {
-#pragma unroll
-        for (int k = 0; k < 5; k++) dFx[k] = 0.0f;
-    }
-    if (edge_y) {
-#pragma unroll
-        for (int k = 0; k < 5; k++) dFy[k] = 0.0f;
-    }
-    float source_rho_e = 0.0f;
+    for (int k = 0; k < 5; k++) n[k] = U[k] - cx * (fR[k] - fL[k]) - cy * (fT[k] - fB[k]);
+    // rho_e source -p div(v) from the face velocities (interior cells only)
     if (interior) {
         float div_v = (uR - uL) * a.inv_dx + (vT - vB) * a.inv_dy;
-        source_rho_e = -p_c * div_v;
+        n[4] += dt * (-p_c * div_v);
     }
-    const float dt = a.dt;
-    float new_rho = U[0] - dt * (dFx[0] + dFy[0]);
-    float new_rho_u = U[1] - dt * (dFx[1] + dFy[1]);
-    float new_rho_v = U[2] - dt * (dFx[2] + dFy[2]);
-    float new_E = U[3] - dt * (dFx[3] + dFy[3]);
-    float new_rho_e = U[4] - dt * (dFx[4] + dFy[4]) + dt * source_rho_e;
+    float new_rho = n[0], new_rho_u = n[1], new_rho_v = n[2], new_E = n[3], new_rho_e = n[4];
     if (!isfinite(new_rho) || new_rho < MIN_DENSITY) new_rho = fmaxf(U[0], MIN_DENSITY);
     if (!isfinite(new_rho_u)) new_rho_u = U[1];
     if (!isfinite(new_rho_v)) new_rho_v = U[2];
     if (!isfinite(new_E)) new_E = U[3];
     if (!isfinite(new_rho_e) || new_rho_e < MIN_PRESSURE / (GAMMA - 1.0f)) new_rho_e = U[4];
     new_rho = fmaxf(new_rho, MIN_DENSITY);
-    float u_new = new_rho_u / new_rho;
-    float v_new = new_rho_v / new_rho;
-    float vel_mag = sqrtf(u_new * u_new + v_new * v_new);
-    if (vel_mag > MAX_VEL) {
-        float scale = MAX_VEL / vel_mag;
+    const float inv_rho = rcp_approx(new_rho);
+    float u_new = new_rho_u * inv_rho;
+    float v_new = new_rho_v * inv_rho;
+    // |u| > MAX_VEL compared in squares; the square root only when rescaling
+    float q = u_new * u_new + v_new * v_new;
+    if (q > MAX_VEL * MAX_VEL) {
+        float scale = MAX_VEL / sqrtf(q);
         u_new *= scale;
         v_new *= scale;
         new_rho_u = new_rho * u_new;
         new_rho_v = new_rho * v_new;
+        q = u_new * u_new + v_new * v_new;
     }
-    float ke = 0.5f * new_rho * (u_new * u_new + v_new * v_new);
-    float eta = (new_E > 0.0f) ? (new_rho_e / new_E) : 1.0f;
-    float e_internal = (eta < ETA_THRESHOLD) ? new_rho_e : (new_E - ke);
-    float e_min = new_rho * R_GAS * MIN_TEMPERATURE / (GAMMA - 1.0f);
-    float e_max = new_rho * R_GAS * MAX_TEMPERATURE / (GAMMA - 1.0f);
-    e_internal = fmaxf(e_internal, e_min);
-    e_internal = fminf(e_internal, e_max);
+    float ke = 0.5f * new_rho * q;
+    float e_internal = dual_energy_low(new_rho_e, new_E) ? new_rho_e : (new_E - ke);
+    constexpr float kEmin = R_GAS * MIN_TEMPERATURE / (GAMMA - 1.0f), kEmax = R_GAS * MAX_TEMPERATURE / (GAMMA - 1.0f);
+    e_internal = fmaxf(e_internal, new_rho * kEmin);
+    e_internal = fminf(e_internal, new_rho * kEmax);
     out[0] = new_rho;
     out[1] = new_rho_u;
     out[2] = new_rho_v;
@@ -536,8 +542,8 @@ __device__ __forceinline__ void ghost_state(float rho_f, float rho_u_f, float rh
 // ------------------------------------------------------------ viscous terms
 // Sutherland viscosity (src/solver.cu:2319, :2351)
 __device__ __forceinline__ float sutherland_mu(float T_val) {
-    float T_ratio = T_val / T_REF;
-    return MU_REF * (T_ratio * sqrtf(T_ratio)) * (T_REF + S_SUTH) / (T_val + S_SUTH);
+    float T_ratio = T_val * (1.0f / T_REF);
+    return MU_REF * (T_ratio * sqrtf(T_ratio)) * (T_REF + S_SUTH) * rcp_approx(T_val + S_SUTH);
 }
 
 // Stress and heat flux at one cell (src/solver.cu:2336-2415) from its 4
@@ -547,13 +553,26 @@ __device__ __forceinline__ float sutherland_mu(float T_val) {
 struct ViscArgs {
     float inv_2dx, inv_2dy, inv_dx, inv_dy, prandtl;
     bool ref_prandtl;
+    float cp_over_pr;  // c_p / Pr (the reference Prandtl number or `prandtl`), set by viscous_args
 };
+// The divisions of a viscous pass computed once: 1/(2dx), 1/dx, ..., c_p / Pr.
+__host__ __device__ __forceinline__ ViscArgs viscous_args(float dx, float dy, float prandtl, bool ref_prandtl) {
+    ViscArgs va;
+    va.inv_2dx = 0.5f / dx;
+    va.inv_2dy = 0.5f / dy;
+    va.inv_dx = 1.0f / dx;
+    va.inv_dy = 1.0f / dy;
+    va.prandtl = prandtl;
+    va.ref_prandtl = ref_prandtl;
+    va.cp_over_pr = ref_prandtl ? CP / PRANDTL_REF : CP / prandtl;
+    return va;
+}
 // `mu_val` is sutherland_mu(TC), computed by the caller.
 __device__ __forceinline__ void stress_heat_mu(float mu_val, float uC, float vC, float TC, float uE, float uW,
                                                float uN, float uS, float vE, float vW, float vN, float vS, float TE,
                                                float TW, float TN, float TS, bool i_lo, bool i_hi, bool j_lo,
                                                bool j_hi, const ViscArgs &va, float out[5]) {
-    float k_val = va.ref_prandtl ? (mu_val * CP / PRANDTL_REF) : (mu_val * CP / va.prandtl);
+    float k_val = mu_val * va.cp_over_pr;
     float du_dx = (uE - uW) * va.inv_2dx;
     float du_dy = (uN - uS) * va.inv_2dy;
     float dv_dx = (vE - vW) * va.inv_2dx;
@@ -597,7 +616,7 @@ __device__ __forceinline__ void stress_heat_mu(float mu_val, float uC, float vC,
 __device__ __forceinline__ void stress_heat_sel(float mu_val, float uE, float uW, float uN, float uS, float vE,
                                                 float vW, float vN, float vS, float TE, float TW, float TN, float TS,
                                                 float fx, float fy, const ViscArgs &va, float out[5]) {
-    float k_val = va.ref_prandtl ? (mu_val * CP / PRANDTL_REF) : (mu_val * CP / va.prandtl);
+    float k_val = mu_val * va.cp_over_pr;
     float du_dx = (uE - uW) * fx;
     float du_dy = (uN - uS) * fy;
     float dv_dx = (vE - vW) * fx;
@@ -619,7 +638,7 @@ __device__ __forceinline__ void stress_heat(float uC, float vC, float TC, float 
 
 // CFL quantities (src/solver.cu:2729-2739, :2679-2687)
 __device__ __forceinline__ float wave_speed(float u, float v, float p, float rho_raw) {
-    float c = sqrtf(GAMMA * p / (rho_raw + 1e-10f));
+    float c = sqrtf(GAMMA * p * rcp_approx(rho_raw + 1e-10f));
     return sqrtf(u * u + v * v) + c;
 }
 

@@ -37,6 +37,8 @@ __device__ __forceinline__ f2 p_max(f2 a, float b) { return mk2(fmaxf(a.x, b), f
 __device__ __forceinline__ f2 p_sqrt(f2 a) { return mk2(sqrtf(a.x), sqrtf(a.y)); }
 // per-lane division a / b, the fast approximate form the scalar path uses
 __device__ __forceinline__ f2 p_div(f2 a, f2 b) { return mk2(__fdividef(a.x, b.x), __fdividef(a.y, b.y)); }
+// per-lane approximate reciprocal, shared by quotients with one divisor
+__device__ __forceinline__ f2 p_rcp(f2 a) { return mk2(rcp_approx(a.x), rcp_approx(a.y)); }
 __device__ __forceinline__ f2 p_sel(bool cx, bool cy, f2 a, f2 b) { return mk2(cx ? a.x : b.x, cy ? a.y : b.y); }
 
 // Limited slope per lane (as limited_slope).
@@ -104,15 +106,18 @@ __device__ __forceinline__ void face_pair_core(bool valid0, bool near0, bool val
     const f2 EL = p_fma(p_mul(hp, rL), qL, eL);
     const f2 ER = p_fma(p_mul(hp, rR), qR, eR);
 
-    // ---- HLLC with Roe-averaged Davis wave speeds
-    const f2 cL = p_sqrt(p_div(p_mul(splat(GAMMA), pL), rL));
-    const f2 cR = p_sqrt(p_div(p_mul(splat(GAMMA), pR), rR));
+    // ---- HLLC with Roe-averaged Davis wave speeds; quotients that share a
+    // divisor (1/rho of each side, the Roe weight sum, the star-state
+    // denominator) multiply by one reciprocal
+    const f2 irL = p_rcp(rL), irR = p_rcp(rR);
+    const f2 cL = p_sqrt(p_mul(p_mul(splat(GAMMA), pL), irL));
+    const f2 cR = p_sqrt(p_mul(p_mul(splat(GAMMA), pR), irR));
     const f2 sqL = p_sqrt(rL), sqR = p_sqrt(rR);
-    const f2 den = p_add(p_add(sqL, sqR), splat(1e-10f));
-    const f2 un_roe = p_div(p_fma(sqL, nL, p_mul(sqR, nR)), den);
-    const f2 ut_roe = p_div(p_fma(sqL, tL, p_mul(sqR, tR)), den);
-    const f2 HL = p_div(p_add(EL, pL), rL), HR = p_div(p_add(ER, pR), rR);
-    const f2 H_roe = p_div(p_fma(sqL, HL, p_mul(sqR, HR)), den);
+    const f2 iden = p_rcp(p_add(p_add(sqL, sqR), splat(1e-10f)));
+    const f2 un_roe = p_mul(p_fma(sqL, nL, p_mul(sqR, nR)), iden);
+    const f2 ut_roe = p_mul(p_fma(sqL, tL, p_mul(sqR, tR)), iden);
+    const f2 HL = p_mul(p_add(EL, pL), irL), HR = p_mul(p_add(ER, pR), irR);
+    const f2 H_roe = p_mul(p_fma(sqL, HL, p_mul(sqR, HR)), iden);
     const f2 q_roe = XDIR ? p_fma(un_roe, un_roe, p_mul(ut_roe, ut_roe)) : p_fma(ut_roe, ut_roe, p_mul(un_roe, un_roe));
     const f2 c2 = p_mul(splat(GAMMA - 1.0f), p_fma(splat(-0.5f), q_roe, H_roe));
     const f2 c_avg = p_mul(hp, p_add(cL, cR));
@@ -142,9 +147,10 @@ __device__ __forceinline__ void face_pair_core(bool valid0, bool near0, bool val
     f2 cd = p_sub(SK, Ss);
     cd = mk2(fabsf(cd.x) < 1e-10f ? (cd.x >= 0.0f ? 1e-10f : -1e-10f) : cd.x,
              fabsf(cd.y) < 1e-10f ? (cd.y >= 0.0f ? 1e-10f : -1e-10f) : cd.y);
-    const f2 rs = p_max(p_div(rkd, cd), MIN_DENSITY);
+    const f2 icd = p_rcp(cd);
+    const f2 rs = p_max(p_mul(rkd, icd), MIN_DENSITY);
     const f2 ps = p_max(p_fma(rkd, p_sub(Ss, nK), pK), MIN_PRESSURE);
-    const f2 Es = p_div(p_sub(p_fma(EK, d, p_mul(ps, Ss)), p_mul(pK, nK)), cd);
+    const f2 Es = p_mul(p_sub(p_fma(EK, d, p_mul(ps, Ss)), p_mul(pK, nK)), icd);
     const bool st0 = !(supL0 || supR0), st1 = !(supL1 || supR1);
     const f2 F0 = p_sel(st0, st1, p_fma(SK, p_sub(rs, rK), fK0), fK0);
     const f2 Fn = p_sel(st0, st1, p_fma(SK, p_sub(p_mul(rs, Ss), fK0), fK1), fK1);
@@ -165,6 +171,30 @@ __device__ __forceinline__ void face_pair_core(bool valid0, bool near0, bool val
     f1[2] = valid1 ? Fy.y : (XDIR ? 0.0f : a.p.y);
     f1[3] = valid1 ? F3.y : 0.0f;
     f1[4] = valid1 ? F4.y : 0.0f;
+}
+
+// Limited x-slopes of a row pair from the slope ring's interleaved entries
+// {rho_r, rho_r+1, u_r, u_r+1}, {v_r, v_r+1, p_r, p_r+1} (x-face frame).
+__device__ __forceinline__ PairSl pair_sl(const float4 &A, const float4 &B) {
+    return PairSl{mk2(A.x, A.y), mk2(A.z, A.w), mk2(B.x, B.y), mk2(B.z, B.w)};
+}
+
+// x-faces of rows r (lane .x -> f0) and r+1 (lane .y -> f1) between cells
+// a | b from their primitives and limited x-slopes sa, sb.
+template <int SCHEME>
+__device__ __forceinline__ void face_pair_x_sl(bool valid0, bool near0, bool valid1, bool near1, const PairPrim &a,
+                                               const PairSl &sa, const PairPrim &b, const PairSl &sb, float f0[5],
+                                               float f1[5]) {
+    if (SCHEME != 0) {  // AUSM+: per lane through the scalar path
+        const float sa0[4] = {sa.rho.x, sa.n.x, sa.t.x, sa.p.x}, sb0[4] = {sb.rho.x, sb.n.x, sb.t.x, sb.p.x};
+        const float sa1[4] = {sa.rho.y, sa.n.y, sa.t.y, sa.p.y}, sb1[4] = {sb.rho.y, sb.n.y, sb.t.y, sb.p.y};
+        face_flux_sl<true, SCHEME>(valid0, near0, Prim{a.rho.x, a.u.x, a.v.x, a.p.x}, sa0,
+                                   Prim{b.rho.x, b.u.x, b.v.x, b.p.x}, sb0, f0);
+        face_flux_sl<true, SCHEME>(valid1, near1, Prim{a.rho.y, a.u.y, a.v.y, a.p.y}, sa1,
+                                   Prim{b.rho.y, b.u.y, b.v.y, b.p.y}, sb1, f1);
+        return;
+    }
+    face_pair_core<true>(valid0, near0, valid1, near1, a, sa, b, sb, f0, f1);
 }
 
 // x-faces of rows r (lane .x -> f0) and r+1 (lane .y -> f1) between cells

@@ -116,16 +116,24 @@ struct StageLayout {
     static constexpr size_t raw_off = 0;
     static constexpr size_t raw_bytes = (size_t)K * SLOT * 4;
     static constexpr size_t bl_off = raw_off + raw_bytes;
-    static constexpr size_t bl_bytes = STAGE == 2 ? (size_t)K * BSLOT * 4 : 0;
+    // stage 2: the blend partner's rows of the row pair updated next, one pair
+    static constexpr size_t bl_bytes = STAGE == 2 ? (size_t)2 * BSLOT * 4 : 0;
     static constexpr size_t p_off = bl_off + bl_bytes;
     static constexpr size_t p_bytes = (size_t)PP * 2 * NT * 16;
-    static constexpr size_t x_off = p_off + p_bytes;
-    static constexpr size_t x_bytes = (size_t)XP * 2 * 6 * NT * 4;  // 5 fluxes + face velocity
+    // x-slopes of the row pair whose x-faces are evaluated next, one pair
+    static constexpr size_t s_off = p_off + p_bytes;
+    static constexpr size_t s_bytes = (size_t)2 * NT * 16;
+    static constexpr size_t x_off = s_off + s_bytes;
+    // per face: {mass, x-mom, y-mom, energy} as a float4 plane, then {rho_e
+    // flux, face velocity} as a float2 plane, one entry per column and row
+    static constexpr size_t x_bytes = (size_t)XP * 2 * NT * (16 + 8);
     static constexpr size_t m_off = x_off + x_bytes;
     static constexpr size_t m_bytes = (size_t)PP * 2 * NT;
     static constexpr size_t bar_off = (m_off + m_bytes + 15) & ~(size_t)15;
-    static constexpr size_t total = bar_off + KP * 8 + 128;  // + alignment slack
-    static constexpr uint32_t tx_bytes = 2 * (5 * BW * 4 + (STAGE == 2 ? 5 * W * 4 : 0));  // one row pair
+    static constexpr int NBAR = KP + (STAGE == 2 ? 1 : 0);  // input pairs + the blend pair
+    static constexpr size_t total = bar_off + NBAR * 8 + 128;  // + alignment slack
+    static constexpr uint32_t tx_bytes = 2 * 5 * BW * 4;       // one input row pair
+    static constexpr uint32_t btx_bytes = 2 * 5 * W * 4;       // one blend row pair
 };
 
 // Slot bookkeeping of a row ring of N slots: rotating the indices of the
@@ -136,10 +144,12 @@ __device__ __forceinline__ int ring_next(int s) {
 }
 
 // TMA ring position carried across the tiles a CTA processes: `base` counts
-// rows staged so far; slot = base % K and the mbarrier phase parity is
-// (base / K) & 1 for the row staged at `base`.
+// input row pairs staged so far (slot = base % KP, mbarrier phase parity
+// (base / KP) & 1 for the pair staged at `base`); `bbase` counts the blend
+// row pairs staged so far (one slot; phase parity bbase & 1).
 struct RingPos {
     int base;
+    int bbase;
 };
 
 // Inviscid SSP-RK2 stage on one tile (strip [i0, i0+W) x rows [j0, j1))
@@ -149,14 +159,20 @@ struct RingPos {
 //   phase 1  primitives + masks of rows r, r+1 (one column per thread)
 //   -- barrier --
 //   phase 2  y-faces (r-2|r-1), (r-1|r) of column i0+t and the update of
-//            rows r-2, r-1 at column i0+t (x-faces of those rows from step q-1)
+//            rows r-2, r-1 at column i0+t (x-faces of those rows from step
+//            q-1); then the limited x-slopes of rows r, r+1 at column i0-1+t
 //   -- barrier --
 //   phase 3  x-faces of rows r, r+1 (thread t: the face left of column i0+t)
+//            from the primitives and x-slopes of the two cells beside it
 // The thread that computes a column's y-faces also updates that column, so
 // y-fluxes stay in registers (the face below row r-2 is carried from the
-// previous step).  After the second barrier nothing reads the previous row
+// previous step).  Every cell's x-slopes are computed once and read by both
+// of its x-faces.  After the second barrier nothing reads the previous row
 // pair's input slot or primitives again, which keeps the rings at K/2 input
-// pairs, 2 primitive pairs and 1 x-face pair.  Returns
+// pairs, 2 primitive pairs, 1 slope pair and 1 x-face pair.  Stage 2 stages
+// the blend partner's rows of pair q into one blend slot after the second
+// barrier of step q (the update of pair q-1 has read the slot by then); the
+// update of pair q in step q+1 waits for them with the input.  Returns
 // false when a bounded wait expired (error recorded; caller must stop).
 template <int NT, int K, int STAGE, int SCHEME, int LIM>
 __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUtensorMap *tm_blend, const StepArgs &a,
@@ -171,9 +187,15 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
     // PB = {v_r, v_r+1, p_r, p_r+1}, one float4 each per column and pair slot
     float4 *PA = reinterpret_cast<float4 *>(smem + L::p_off);
     float4 *PB = PA + L::PP * NT;
-    float *X = reinterpret_cast<float *>(smem + L::x_off);
+    // x-slopes of a row pair, interleaved like the primitives (face frame:
+    // normal u, tangential v): SA = {rho_r, rho_r+1, u_r, u_r+1}, SB = {v, p}
+    float4 *SA = reinterpret_cast<float4 *>(smem + L::s_off);
+    float4 *SB = SA + NT;
+    float4 *X4 = reinterpret_cast<float4 *>(smem + L::x_off);  // [row h][column]
+    float2 *X2 = reinterpret_cast<float2 *>(X4 + 2 * NT);       // [row h][column]
     uint8_t *M = smem + L::m_off;
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bar_off);
+    uint64_t *bbar = bars + KP;  // blend pair (stage 2)
 
     const GridDesc g = a.g;
     const int nx = g.nx, ny = g.ny;
@@ -188,6 +210,7 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
     fence_proxy_async_smem();
     __syncthreads();
     const int base = rp.base;  // row pairs this CTA staged before this tile
+    const int bbase = rp.bbase;
     int islot = base % KP;
     auto issue = [&](int q) {
         mbar_arrive_expect_tx(&bars[islot], L::tx_bytes);
@@ -198,10 +221,19 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
 #pragma unroll
             for (int b = 0; b < L::NB; b++)
                 tma_load_3d(dst + b * kBoxStride, tm_in, &bars[islot], i0 - 4 + b * kBox, row, 0);
-            if (STAGE == 2)
-                tma_load_3d(bl + (size_t)(islot * 2 + h) * L::BSLOT, tm_blend, &bars[islot], i0, row, 0);
         }
         islot = ring_next<KP>(islot);
+    };
+    // blend partner rows of pair p (updated in step p+1; pair 0 and the last
+    // pair are never updated)
+    const int nblend = STAGE == 2 ? max(0, npairs - 2) : 0;
+    int bissued = 0;  // blend pairs staged in this tile (thread 0's count)
+    auto issue_blend = [&](int p) {
+        ++bissued;
+        mbar_arrive_expect_tx(bbar, L::btx_bytes);
+#pragma unroll
+        for (int h = 0; h < 2; h++)
+            tma_load_3d(bl + (size_t)h * L::BSLOT, tm_blend, bbar, i0, clampi(rs + 2 * p + h, 0, ny - 1), 0);
     };
     int issued = min(KP, npairs);
     if (t == 0)
@@ -233,6 +265,7 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
         // ---- phase 1: primitives + masks of rows r, r+1
         const int s0 = pc0 >> 1, s1 = pc1 >> 1;  // pair slots of q, q-1
         bool ok = mbar_wait_bounded(&bars[kr], (uint32_t)par);
+        if (STAGE == 2 && q >= 2) ok = ok && mbar_wait_bounded(bbar, (uint32_t)((bbase + q - 2) & 1));
         if (ok) {
             float rho[2], u[2], v[2], p[2];
 #pragma unroll
@@ -278,6 +311,7 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
             if (urow >= j0 && urow < j1 && col_ok) {
                 const uint32_t mb = M[(pc1 + h) * NT + cy];
                 const float *src = raw + (size_t)(ku * 2 + h) * L::SLOT;
+                const bool edge_y = (urow == 0 || urow == ny - 1);
                 float Uc[5], Un[5];
 #pragma unroll
                 for (int k = 0; k < 5; k++) Uc[k] = ring_at<L::NB>(src, k, t + 4);
@@ -285,28 +319,30 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
 #pragma unroll
                     for (int k = 0; k < 5; k++) Un[k] = Uc[k];
                 } else {
-                    const float *Xs = X + h * 6 * NT + t;
-                    float fR[5], fL[5], fT[5], fB[5];
+                    const float4 L4 = X4[h * NT + t], R4 = X4[h * NT + t + 1];
+                    const float2 L2 = X2[h * NT + t], R2 = X2[h * NT + t + 1];
+                    const float fR[5] = {R4.x, R4.y, R4.z, R4.w, R2.x};
+                    const float fL[5] = {L4.x, L4.y, L4.z, L4.w, L2.x};
+                    float fT[5], fB[5];
 #pragma unroll
                     for (int k = 0; k < 5; k++) {
-                        fR[k] = Xs[k * NT + 1];
-                        fL[k] = Xs[k * NT];
                         fT[k] = h ? fy1[k] : fy0[k];
                         fB[k] = h ? fy0[k] : fyB[k];
                     }
                     const float4 pc = h ? c1 : c2;
                     const float vT = h ? vf1 : vf0, vB = h ? vf0 : vfB;
-                    const bool edge_y = (urow == 0 || urow == ny - 1);
-                    update_cell(Uc, fR, fL, fT, fB, Xs[5 * NT + 1], Xs[5 * NT], vT, vB, pc.w, edge_x, edge_y,
-                                !edge_x && !edge_y, ua, Un);
+                    update_cell(Uc, fR, fL, fT, fB, R2.y, L2.y, vT, vB, pc.w, edge_x, edge_y, !edge_x && !edge_y,
+                                ua, Un);
                 }
                 if (STAGE == 2) {
-                    const float *b = bl + (size_t)(ku * 2 + h) * L::BSLOT + t;
+                    const float *b = bl + (size_t)h * L::BSLOT + t;
 #pragma unroll
                     for (int k = 0; k < 5; k++) Un[k] = 0.5f * b[k * W] + 0.5f * Un[k];
                 }
                 const uint32_t ctype = mb_type(mb);
-                if (a.apply_bc) bc_pointwise(Un, ctype, iu, urow, nx, ny, a.fs);
+                // phase-1 conditions act only on non-fluid cells and the domain's edge cells
+                if (a.apply_bc && (ctype != CT_FLUID || edge_x || edge_y))
+                    bc_pointwise(Un, ctype, iu, urow, nx, ny, a.fs);
                 if (a.cfl && ctype != CT_GHOST) {
                     float uu, vv, pp, TT;
                     prim_from_cons(Un[0], Un[1], Un[2], Un[3], Un[4], uu, vv, pp, TT);
@@ -321,31 +357,41 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
 #pragma unroll
         for (int k = 0; k < 5; k++) fyB[k] = fy1[k];
         vfB = vf1;
+        // x-slopes of rows r, r+1 at staged column t+1 (columns 1 .. NT-2 are
+        // the cells beside the x-faces of phase 3)
+        if (t < NT - 2) {
+            const float4 *A = PA + s0 * NT + t, *B = PB + s0 * NT + t;
+            const PairPrim m = pair_prim(A[0], B[0]), c = pair_prim(A[1], B[1]), p = pair_prim(A[2], B[2]);
+            const f2 sr = p_slope<LIM>(m.rho, c.rho, p.rho), su = p_slope<LIM>(m.u, c.u, p.u);
+            const f2 sv = p_slope<LIM>(m.v, c.v, p.v), sp = p_slope<LIM>(m.p, c.p, p.p);
+            SA[t + 1] = make_float4(sr.x, sr.y, su.x, su.y);
+            SB[t + 1] = make_float4(sv.x, sv.y, sp.x, sp.y);
+        }
         fence_proxy_async_smem();
         __syncthreads();
-        // the input slot of pair q-1 is free now: stage pair q-1+KP into it
-        if (t == 0 && issued < npairs && issued <= q + KP - 1) {
-            issue(issued);
-            ++issued;
+        // the input slot of pair q-1 is free now: stage pair q-1+KP into it;
+        // the blend slot too: stage the blend rows of pair q
+        if (t == 0) {
+            if (issued < npairs && issued <= q + KP - 1) {
+                issue(issued);
+                ++issued;
+            }
+            if (STAGE == 2 && q >= 1 && q <= nblend) issue_blend(q);
         }
         // ---- phase 3: x-faces of rows r, r+1 (read by the update in step q+1)
         {
             float fx0[5], fx1[5];
             const float4 *A = PA + s0 * NT, *B = PB + s0 * NT;
             const uint32_t mb0 = M[pc0 * NT + tx + 1], mb1 = M[(pc0 + 1) * NT + tx + 1];
-            face_pair_x<SCHEME, LIM>((mb0 & MB_XV) != 0, (mb0 & MB_XN) != 0, (mb1 & MB_XV) != 0, (mb1 & MB_XN) != 0,
-                                     pair_prim(A[tx], B[tx]), pair_prim(A[tx + 1], B[tx + 1]),
-                                     pair_prim(A[tx + 2], B[tx + 2]), pair_prim(A[tx + 3], B[tx + 3]), fx0, fx1);
+            face_pair_x_sl<SCHEME>((mb0 & MB_XV) != 0, (mb0 & MB_XN) != 0, (mb1 & MB_XV) != 0, (mb1 & MB_XN) != 0,
+                                   pair_prim(A[tx + 1], B[tx + 1]), pair_sl(SA[tx + 1], SB[tx + 1]),
+                                   pair_prim(A[tx + 2], B[tx + 2]), pair_sl(SA[tx + 2], SB[tx + 2]), fx0, fx1);
             if (t <= W) {
-                float *Xs = X + t;
-#pragma unroll
-                for (int k = 0; k < 5; k++) {
-                    Xs[k * NT] = fx0[k];
-                    Xs[(6 + k) * NT] = fx1[k];
-                }
-                // face velocities for the rho_e source of both adjacent cells
-                Xs[5 * NT] = face_velocity(fx0[0], A[tx + 1].x, A[tx + 2].x);
-                Xs[11 * NT] = face_velocity(fx1[0], A[tx + 1].y, A[tx + 2].y);
+                X4[t] = make_float4(fx0[0], fx0[1], fx0[2], fx0[3]);
+                X4[NT + t] = make_float4(fx1[0], fx1[1], fx1[2], fx1[3]);
+                // with the face velocities for the rho_e source of both adjacent cells
+                X2[t] = make_float2(fx0[4], face_velocity(fx0[0], A[tx + 1].x, A[tx + 2].x));
+                X2[NT + t] = make_float2(fx1[4], face_velocity(fx1[0], A[tx + 1].y, A[tx + 2].y));
             }
         }
         pc1 = pc0;
@@ -360,10 +406,14 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
             // drain loads still in flight before the shared memory is released
             for (int q = 0; q < issued; q++)
                 mbar_wait_bounded(&bars[(base + q) % KP], (uint32_t)(((base + q) / KP) & 1), 20000000LL);
+            // each blend pair is consumed one step after it is staged, so at
+            // most the last one staged can still be in flight
+            if (bissued > 0) mbar_wait_bounded(bbar, (uint32_t)((bbase + bissued - 1) & 1), 20000000LL);
         }
         return false;
     }
     rp.base = base + npairs;
+    rp.bbase = bbase + nblend;
     return true;
 }
 
@@ -382,10 +432,10 @@ __global__ void __launch_bounds__(NT, 768 / NT)
     if (threadIdx.x == 0) {
         prefetch_tensormap(&tm_in);
         if (STAGE == 2) prefetch_tensormap(&tm_blend);
-        for (int k = 0; k < L::KP; k++) mbar_init(&bars[k], 1);
+        for (int k = 0; k < L::NBAR; k++) mbar_init(&bars[k], 1);
         fence_barrier_init();
     }
-    RingPos rp{0};
+    RingPos rp{0, 0};
     float lmax = 0.0f;
     unsigned nbad = 0;
     if (!stage_tile<NT, K, STAGE, SCHEME, LIM>(&tm_in, &tm_blend, a, blockIdx.x * L::W, blockIdx.y * a.rows_per_cta,
@@ -407,8 +457,10 @@ struct ViscLayout {
     static constexpr size_t raw_bytes = (size_t)K * SLOT * 4;
     static constexpr size_t p_off = raw_off + raw_bytes;
     static constexpr size_t p_bytes = (size_t)PP * 2 * NT * 16;
+    // stress / heat flux per (row, column): {txx, tyy, txy, qx} in a float4
+    // plane, qy in a float plane
     static constexpr size_t t_off = p_off + p_bytes;
-    static constexpr size_t t_bytes = (size_t)TP * 2 * 5 * NT * 4;
+    static constexpr size_t t_bytes = (size_t)TP * 2 * NT * (16 + 4);
     static constexpr size_t m_off = t_off + t_bytes;
     static constexpr size_t m_bytes = (size_t)PP * 2 * NT;
     static constexpr size_t bar_off = (m_off + m_bytes + 15) & ~(size_t)15;
@@ -438,8 +490,9 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
     constexpr int KP = L::KP;
     static_assert(L::PP == 3 && L::TP == 2 && KP >= 2, "ring sizes");
     float *raw = reinterpret_cast<float *>(smem + L::raw_off);
-    float4 *P = reinterpret_cast<float4 *>(smem + L::p_off);  // {u, v, T, mu}
-    float *Tq = reinterpret_cast<float *>(smem + L::t_off);   // {txx, tyy, txy, qx, qy}
+    float4 *P = reinterpret_cast<float4 *>(smem + L::p_off);     // {u, v, T, mu}
+    float4 *T4 = reinterpret_cast<float4 *>(smem + L::t_off);    // {txx, tyy, txy, qx}, [row][column]
+    float *T1 = reinterpret_cast<float *>(T4 + L::TP * 2 * NT);  // qy, [row][column]
     uint8_t *M = smem + L::m_off;
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bar_off);
 
@@ -450,13 +503,7 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
     const int rs = j0 - 2;
     const int npairs = (j1 - j0 + 5) / 2;  // incoming rows rs .. j1+1 (one spare row when odd)
     const float dt = a.sc->dt * a.dt_scale;
-    ViscArgs va;
-    va.inv_2dx = 0.5f / g.dx;
-    va.inv_2dy = 0.5f / g.dy;
-    va.inv_dx = 1.0f / g.dx;
-    va.inv_dy = 1.0f / g.dy;
-    va.prandtl = a.prandtl;
-    va.ref_prandtl = a.ref_prandtl != 0;
+    const ViscArgs va = viscous_args(g.dx, g.dy, a.prandtl, a.ref_prandtl != 0);
 
     fence_proxy_async_smem();
     __syncthreads();
@@ -567,9 +614,8 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
             }
 #pragma unroll
             for (int h = 0; h < 2; h++) {
-                float *Ts = Tq + (tc0 + h) * 5 * NT + t;
-#pragma unroll
-                for (int k = 0; k < 5; k++) Ts[k * NT] = out[h][k];
+                T4[(tc0 + h) * NT + t] = make_float4(out[h][0], out[h][1], out[h][2], out[h][3]);
+                T1[(tc0 + h) * NT + t] = out[h][4];
             }
         }
         // south neighbour of row r-2 (row r-3, pair q-2): read before its slot is reused
@@ -587,20 +633,15 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
                 const int prow = pc1 + h;
                 store[h] = col_ok && urow >= j0 && urow < j1;
                 ctype[h] = mb_type(M[prow * NT + tp]);
-                // stress rows urow-1, urow, urow+1
+                // stress rows urow-1, urow, urow+1 (qy only of the north and south rows)
                 const int tS = h ? tc1 + 1 : tc1, tC0 = h ? tc0 : tc1 + 1, tN = h ? tc0 + 1 : tc0;
-                const float *T0 = Tq + tC0 * 5 * NT + tp;
-                const float *TN = Tq + tN * 5 * NT + tp;
-                const float *TS = Tq + tS * 5 * NT + tp;
-                float tC[5], tE[5], tW[5], tNn[5], tSs[5];
-#pragma unroll
-                for (int k = 0; k < 5; k++) {
-                    tC[k] = T0[k * NT];
-                    tE[k] = T0[k * NT + 1];
-                    tW[k] = T0[k * NT - 1];
-                    tNn[k] = TN[k * NT];
-                    tSs[k] = TS[k * NT];
-                }
+                const float4 C4 = T4[tC0 * NT + tp], E4 = T4[tC0 * NT + tp + 1], W4 = T4[tC0 * NT + tp - 1];
+                const float4 N4 = T4[tN * NT + tp], S4 = T4[tS * NT + tp];
+                const float tC[5] = {C4.x, C4.y, C4.z, C4.w, 0.0f};
+                const float tE[5] = {E4.x, E4.y, E4.z, E4.w, 0.0f};
+                const float tW[5] = {W4.x, W4.y, W4.z, W4.w, 0.0f};
+                const float tNn[5] = {N4.x, N4.y, N4.z, N4.w, T1[tN * NT + tp]};
+                const float tSs[5] = {S4.x, S4.y, S4.z, S4.w, T1[tS * NT + tp]};
                 const float4 E = P[prow * NT + tp + 1], Wc = P[prow * NT + tp - 1];
                 const float4 N = P[(h ? pc0 : pc1 + 1) * NT + tp];
                 const float4 S = h ? P[pc1 * NT + tp] : S0;
@@ -614,7 +655,11 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
             }
             if (a.apply_bc) {
 #pragma unroll
-                for (int h = 0; h < 2; h++) bc_pointwise(U[h], ctype[h], ic, r - 2 + h, nx, ny, a.fs);
+                for (int h = 0; h < 2; h++) {
+                    const int row = r - 2 + h;
+                    if (ctype[h] != CT_FLUID || !interior_x || row == 0 || row == ny - 1)
+                        bc_pointwise(U[h], ctype[h], ic, row, nx, ny, a.fs);
+                }
             }
             if (a.cfl) {
 #pragma unroll
@@ -627,7 +672,7 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
                     nbad += counted ? nonfinite5(U[h]) : 0u;
                     if (a.cfl == 2) {
                         const float mu = (ctype[h] == CT_SOLID) ? 0.0f : P[(pc1 + h) * NT + tp].w;
-                        const float nu = mu / (U[h][0] + 1e-10f);
+                        const float nu = mu * rcp_approx(U[h][0] + 1e-10f);
                         lmax_nu = counted ? fmaxf(lmax_nu, nu) : lmax_nu;
                     }
                 }
@@ -678,7 +723,7 @@ __global__ void __launch_bounds__(NT, 768 / NT) k_viscous(const __grid_constant_
         for (int k = 0; k < L::KP; k++) mbar_init(&bars[k], 1);
         fence_barrier_init();
     }
-    RingPos rp{0};
+    RingPos rp{0, 0};
     float ls = 0.0f, ln = 0.0f;
     unsigned nbad = 0;
     if (!viscous_tile<NT, K>(&tm_in, a, blockIdx.x * L::W, blockIdx.y * a.rows_per_cta, smem, rp, ls, ln, nbad))
@@ -727,10 +772,10 @@ __global__ void __launch_bounds__(NT, 640 / NT) k_stage_batch(const BatchInst *_
     if (smem_misaligned(smem, insts[0].sc)) return;
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bar_off);
     if (threadIdx.x == 0) {
-        for (int k = 0; k < L::KP; k++) mbar_init(&bars[k], 1);
+        for (int k = 0; k < L::NBAR; k++) mbar_init(&bars[k], 1);
         fence_barrier_init();
     }
-    RingPos rp{0};
+    RingPos rp{0, 0};
     for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
         const TileDesc td = tiles[ti];
         const BatchInst &I = insts[td.inst];
@@ -776,7 +821,7 @@ __global__ void __launch_bounds__(NT, 640 / NT) k_viscous_batch(const BatchInst 
         for (int k = 0; k < L::KP; k++) mbar_init(&bars[k], 1);
         fence_barrier_init();
     }
-    RingPos rp{0};
+    RingPos rp{0, 0};
     for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
         const TileDesc td = tiles[ti];
         const BatchInst &I = insts[td.inst];

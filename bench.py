@@ -52,6 +52,9 @@ BATCH_SEED, SERVE_SEED = 4, 5
 # blend partner read once.
 KERNEL_BYTES = {"stage1": 41, "stage2": 61, "viscous_pre": 41, "viscous_post": 41}
 STEP_BYTES_FUSED = 102  # compulsory bytes per cell-update of a fused 5-field RK2 step
+# Navier-Stokes: the two Strang viscous half steps are passes of their own
+# (41 B each: state in, state out, mask)
+STEP_BYTES_NS = 184
 # DRAM bytes (read + write) per launch measured by ncu on the 4096x2048 case
 # and scaled by the cell count to 8192x4096 (profiles/marching_kernels_*.md).
 MEASURED_TRAFFIC = {
@@ -284,16 +287,38 @@ def bench_batched(n_inst=256, steps=20, warmup=5, solo_steps=10):
     }
 
 
-def bench_serving(lams=(10.0, 100.0, 1000.0), n_req=24, chunk=64, budget=150 * 10**9, class_steps=20):
-    """Continuous-batching request loop on Poisson arrivals; the one-at-a-time
-    comparison is a FIFO single-solve queue on the same arrivals, each request
-    served at the measured single-solve rate of its grid/physics class."""
+def one_at_a_time(torch, fvm_b200, reqs, ext, stream):
+    """The same arrivals served one solve at a time on this GPU, first come
+    first served: each request waits for its arrival and for the previous
+    solve, then a single-solve handle is created, stepped, its FP64
+    diagnostics read to the host and the handle destroyed.  Wall-clock times
+    like the server's.  Returns (sorted completion latencies, span, work)."""
+    t0 = time.perf_counter()
+    lat, work, done = [], 0, 0.0
+    for t, p, n in reqs:
+        now = time.perf_counter() - t0
+        if now < t:
+            time.sleep(t - now)
+        s = fvm_b200.Solver(abi.SimParams.from_buffer_copy(p), ext)
+        s.set_stream(stream.cuda_stream)
+        s.step(n)
+        s.diagnostics()
+        s.close()
+        done = time.perf_counter() - t0
+        lat.append(done - t)
+        work += p.nx * p.ny * n
+    return sorted(lat), done - reqs[0][0], work
+
+
+def bench_serving(lams=(10.0, 100.0, 1000.0), n_req=48, chunk=64, budget=150 * 10**9, class_steps=20):
+    """Continuous-batching request loop on Poisson arrivals, against the same
+    arrivals served one solve at a time on the same GPU (measured)."""
     import torch
     import fvm_b200
     stream = torch.cuda.Stream()
     ext = abi.ext_default()
     ext.dt_policy = abi.DT_RECOMPUTE
-    # single-solve rate per (grid, viscous) class
+    # single-solve rate per (grid, viscous) class: what batching can gain on a mix
     class_rate = {}
     rng = abi.SeededStream(SERVE_SEED + 1)
     for nx in (256, 512, 1024, 2048):
@@ -304,6 +329,7 @@ def bench_serving(lams=(10.0, 100.0, 1000.0), n_req=24, chunk=64, budget=150 * 1
                     break
             ms = solo_rate(torch, fvm_b200, p, ext, stream, class_steps)
             class_rate[(nx, visc)] = p.nx * p.ny * class_steps / (ms / 1e3)
+    q = lambda v, f: v[min(len(v) - 1, int(round(f * (len(v) - 1))))] if v else None  # noqa: E731
     sweep = []
     for lam in lams:
         reqs = serving_requests(n_req, lam)
@@ -329,16 +355,10 @@ def bench_serving(lams=(10.0, 100.0, 1000.0), n_req=24, chunk=64, budget=150 * 1
         work = sum(r.nx * r.ny * r.steps for r in ok)
         span = max(r.done_s for r in res) - min(r.submit_s for r in res)
         lat = sorted(r.done_s - r.submit_s for r in ok)
-        # one at a time: FIFO queue, service = work / class rate
-        free_at, solo_lat = 0.0, []
-        for t, p, n in reqs:
-            start = max(t, free_at)
-            free_at = start + p.nx * p.ny * n / class_rate[(p.nx, bool(p.enable_viscosity))]
-            solo_lat.append(free_at - t)
-        solo_lat.sort()
-        solo_span = free_at - reqs[0][0]
-        solo_work = sum(p.nx * p.ny * n for _, p, n in reqs)
-        q = lambda v, f: v[min(len(v) - 1, int(round(f * (len(v) - 1))))] if v else None  # noqa: E731
+        solo_lat, solo_span, solo_work = one_at_a_time(torch, fvm_b200, reqs, ext, stream)
+        # every request at its class's single-solve rate: the work-weighted
+        # single-solve rate, the one-at-a-time rate without set-up or idle time
+        solo_model_s = sum(p.nx * p.ny * n / class_rate[(p.nx, bool(p.enable_viscosity))] for _, p, n in reqs)
         sweep.append({
             "lambda_per_s": lam, "requests": n_req, "completed_ok": len(ok), "failed": len(res) - len(ok),
             "value": work / span, "unit": "cell-updates/s",
@@ -347,13 +367,56 @@ def bench_serving(lams=(10.0, 100.0, 1000.0), n_req=24, chunk=64, budget=150 * 1
             "device_busy_frac": st.busy_s / span,
             "one_at_a_time": {"value": solo_work / solo_span, "unit": "cell-updates/s",
                               "completion_s_p50": q(solo_lat, 0.5), "completion_s_p99": q(solo_lat, 0.99),
-                              "model": "FIFO single-solve queue on the same arrivals at measured per-class rates"},
+                              "measured": "same arrivals, one single-solve handle at a time, FIFO, wall clock"},
             "speedup_vs_one_at_a_time": (work / span) / (solo_work / solo_span),
+            "single_solve_rate_work_weighted": solo_work / solo_model_s,
             "batched_steps": st.batched_steps,
         })
     return {"sweep": sweep, "class_rates": {f"{k[0]}x{k[0] // 2}{'_ns' if k[1] else '_euler'}": v
                                             for k, v in class_rate.items()},
             "budget_bytes": budget, "chunk_steps": chunk}
+
+
+def reference_cuda(grids=((8192, 4096), (1024, 512)), steps=20):
+    """The reference's own FP32 CUDA KernelBenchmark (src/test/kernel_benchmark.cu,
+    built unmodified from the reference sources into oracle/_ref/) beside the
+    same case through this library's CFDSolver shim, on this GPU: ms per step
+    of each (each program's own host-clock timing of its timed steps), with
+    the clocks seen."""
+    ref_bin = os.path.join(REPO, "oracle", "_ref", "kernel_benchmark")
+    own_bin = os.path.join(PKG, "fvm_b200", "lib", "kernel_benchmark")
+    if not (os.path.exists(ref_bin) and os.path.exists(own_bin)):
+        return {"unavailable": "reference KernelBenchmark or shim benchmark not built"}
+
+    def avg_ms(cmd):
+        # the reference prints "Total time: X ms" over "Running benchmark (N
+        # steps)" with two decimals; the total keeps more of them than its
+        # per-step line.  The shim prints "Avg per step: X ms" with four.
+        out = subprocess.run(cmd, capture_output=True, text=True, timeout=300)
+        total, n, avg = None, None, None
+        for ln in out.stdout.splitlines():
+            ln = ln.strip()
+            if ln.startswith("Total time:"):
+                total = float(ln.split()[2])
+            elif "Running benchmark (" in ln:
+                n = int(ln.split("(")[1].split()[0])
+            elif ln.startswith("Avg per step:"):
+                avg = float(ln.split()[3])
+        if total is not None and n:
+            return total / n
+        if avg is not None:
+            return avg
+        raise RuntimeError(f"{cmd[0]}: no timing line (rc {out.returncode}): {out.stderr[-200:]}")
+
+    clocks = ClockSampler(0)
+    clocks.start()
+    rows = []
+    for nx, ny in grids:
+        r = avg_ms([ref_bin, str(nx), str(ny)])
+        o = avg_ms([own_bin, str(nx), str(ny), str(steps)])
+        rows.append({"grid": f"{nx}x{ny}", "reference_ms_per_step": r, "this_ms_per_step": o, "speedup": r / o})
+    return {"case": "reference KernelBenchmark: NS Mach 3 circle, HLLC + minmod, fixed dt, one step() per step",
+            "rows": rows, "clocks": clocks.stop()}
 
 
 def run_reference_arm(args, params, ext, ws, rank, dist):
@@ -561,7 +624,7 @@ def main():
     ap.add_argument("--no-extras", action="store_true",
                     help="default workload only: skip the batched and serving summaries")
     ap.add_argument("--instances", type=int, default=256, help="batched_uneven: number of solves")
-    ap.add_argument("--requests", type=int, default=96, help="serving: requests per arrival rate")
+    ap.add_argument("--requests", type=int, default=48, help="serving: requests per arrival rate")
     ap.add_argument("--lambdas", default="10,100,1000", help="serving: arrival rates [1/s]")
     args = ap.parse_args()
     assert args.warmup >= 3, "at least 3 warm-up steps"
@@ -593,11 +656,14 @@ def main():
     import fvm_b200
     torch.cuda.set_device(local)
     stream = torch.cuda.Stream()
+    # every step takes the CFL time step of its own start state (reduced on
+    # the device, fused into the step's last kernels): the flow stays within
+    # the stability limit while the bow shock forms
+    ext.dt_policy = abi.DT_RECOMPUTE
     s = fvm_b200.Solver(params, ext)
     s.set_stream(stream.cuda_stream)
     with torch.cuda.stream(stream):
-        # settle into a non-uniform flow, fixed dt from the start state
-        params.dt = s.compute_dt()
+        # settle into a non-uniform flow
         s.step(args.settle)
         if not args.no_autotune:
             s.autotune(steps=4)  # launch shape for this grid class (untimed)
@@ -643,13 +709,55 @@ def main():
         cmap_ms = c0.elapsed_time(c1) / 10
         del img
 
-        # ---- end to end through the C ABI with host buffers: upload state,
-        # K steps, download state
+        # ---- end to end through the C ABI, the reference application's
+        # frame loop (src/main.cpp:285-367, one step per frame): step with the
+        # time step read back at the end of the previous frame, the Mach
+        # field into a device buffer (the display buffer), maximum
+        # temperature and Mach number to the host at most every 0.25 s (the
+        # first frame included), the next time step queued and read back
+        # (which waits for the frame's work)
         import ctypes as C
+        lib = s.lib
+        e_fixed = abi.Ext.from_buffer_copy(ext)
+        e_fixed.dt_policy = abi.DT_FIXED
+        s.set_ext(e_fixed)
+        field = torch.empty(nx * ny, dtype=torch.float32, device="cuda")
+        dt_c, tmax, mmax = C.c_float(), C.c_float(), C.c_float()
+        stats_reads = [0, -1.0]
+
+        def frame():
+            s.params.dt = dt_c.value
+            fvm_b200._check(lib.fvm_steps(s.h, C.byref(s.params), 1))
+            fvm_b200._check(lib.fvm_field_to_device(s.h, abi.FIELD_MACH, C.c_void_p(field.data_ptr())))
+            now = time.perf_counter()
+            if stats_reads[1] < 0 or now - stats_reads[1] >= 0.25:
+                fvm_b200._check(lib.fvm_max_temperature(s.h, C.byref(tmax)))
+                fvm_b200._check(lib.fvm_max_mach(s.h, C.byref(mmax)))
+                stats_reads[0] += 1
+                stats_reads[1] = now
+            fvm_b200._check(lib.fvm_queue_dt(s.h, C.byref(s.params)))
+            fvm_b200._check(lib.fvm_read_dt(s.h, C.byref(s.params), C.byref(dt_c)))
+
+        fvm_b200._check(lib.fvm_compute_dt(s.h, C.byref(s.params), C.byref(dt_c)))
+        for _ in range(args.warmup):
+            frame()
+        barrier(dist)
+        torch.cuda.synchronize()
+        stats_reads[:] = [0, -1.0]
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            frame()
+        app_s = time.perf_counter() - t0
+        app_stats_reads = stats_reads[0]
+        app_max = max_over_ranks(app_s, dist)
+        assert np.isfinite(tmax.value) and np.isfinite(mmax.value) and dt_c.value > 0
+        s.set_ext(ext)
+
+        # ---- end to end with the whole state through host memory: upload
+        # the state from pinned host buffers, K steps, download the state
         U = s.fields()
         host = [torch.from_numpy(np.ascontiguousarray(U[k])).pin_memory() for k in range(5)]
         out = [torch.empty_like(h).pin_memory() for h in host]
-        lib = s.lib
         barrier(dist)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -663,6 +771,7 @@ def main():
     cells = nx * ny
     value = cells * args.steps * ws / (ms_max / 1e3)
     e2e_value = cells * args.steps * ws / e2e_max
+    app_value = cells * args.steps * ws / app_max
     hbm, peak_kind = load_peaks()
     # dominant kernel by total time
     dom = max(((k, v) for k, v in ktimes.items() if k in KERNEL_BYTES), key=lambda kv: kv[1][1])
@@ -675,13 +784,15 @@ def main():
         budget = float(os.environ.get("FVM_CPU_BUDGET_S", "15"))
         r, threads, sample = cpu_reference(params, ext, steps_budget_s=budget)
         cpu = {"value": r, "unit": "cell-updates/s", "cores": threads, "kind": "port", "sample": sample}
-    step_gbs = value / ws * STEP_BYTES_FUSED / 1e9
+    step_bytes = STEP_BYTES_NS if params.enable_viscosity else STEP_BYTES_FUSED
+    step_gbs = value / ws * step_bytes / 1e9
     tune = dict(zip(("threads", "ring", "rows_per_cta"), s.tune()))
     s.close()
     extras = {}
     if rank == 0 and ws == 1 and not args.no_extras:
-        for name, fn in (("batched", lambda: bench_batched(n_inst=args.instances, steps=10, warmup=args.warmup)),
-                         ("serving", lambda: bench_serving(lams=(100.0,), n_req=16))):
+        for name, fn in (("reference_cuda", reference_cuda),
+                         ("batched", lambda: bench_batched(n_inst=args.instances, steps=10, warmup=args.warmup)),
+                         ("serving", lambda: bench_serving(lams=(10.0, 100.0, 1000.0), n_req=args.requests))):
             try:
                 extras[name] = fn()
             except Exception as exc:  # reported, never hides the main line
@@ -697,14 +808,24 @@ def main():
                        "flux": ["hllc", "ausm+"][ext.flux_scheme], "limiter": ["minmod", "van_leer"][ext.limiter],
                        "parallelism": f"replicas x{ws}", "l2": "inputs > L2 (670 MB per state), no flush",
                        "tune": tune},
-            "hbm_gbs_per_gpu_at_102B": step_gbs,
+            "step_hbm": {"gbs_per_gpu": step_gbs, "algorithmic_bytes_per_cell": step_bytes,
+                         "frac": step_gbs / hbm,
+                         "basis": "whole step: 5 conserved fields in and out of every pass, mask bytes"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": traffic, "kernel": dom_name,
                          "algorithmic_bytes_per_cell": KERNEL_BYTES[dom_name], "peak_kind": peak_kind},
             "kernels": {k: {"launches": v[0], "avg_ms": v[1] / v[0]} for k, v in ktimes.items()},
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e_value, "unit": "cell-updates/s",
-                    "h2d_bytes_per_step": cells * 20 / args.steps, "d2h_bytes_per_step": cells * 20 / args.steps},
+            "e2e": {"value": app_value, "unit": "cell-updates/s", "h2d_bytes_per_step": 4,
+                    "d2h_bytes_per_step": 4 + 8 * app_stats_reads / args.steps,
+                    "ms_per_frame": app_max / args.steps * 1e3,
+                    "protocol": "reference app frame loop, one step per frame: fvm_steps(1) with the host's dt "
+                                "(4 B in), Mach field into a device buffer, max T and max Mach to host every "
+                                "0.25 s, fvm_queue_dt + fvm_read_dt (dt to host, waits for the frame)"},
+            "e2e_state_roundtrip": {"value": e2e_value, "unit": "cell-updates/s", "steps_per_roundtrip": args.steps,
+                                    "h2d_bytes_per_step": cells * 20 / args.steps,
+                                    "d2h_bytes_per_step": cells * 20 / args.steps,
+                                    "includes": "whole state from pinned host memory, K steps, whole state back"},
             "gpu_launches": launches,
             "clocks": clk,
             # Mach field (reads rho, rho_u, rho_v, rho_e = 16 B + class 1 B, writes 4 B per cell)

@@ -217,16 +217,6 @@ __device__ __forceinline__ void ausm_plus_flux(float rhoL, float unL, float utL,
     f[3] = a * rhoL * HL + b * rhoR * HR;
 }
 
-// Limited slopes of cell c from its neighbours m and p along one direction,
-// in the face frame (rho, normal velocity, tangential velocity, p).
-template <bool XDIR, int LIM>
-__device__ __forceinline__ void cell_slopes(const Prim &m, const Prim &c, const Prim &p, float s[4]) {
-    s[0] = limited_slope<LIM>(m.rho, c.rho, p.rho);
-    s[1] = XDIR ? limited_slope<LIM>(m.u, c.u, p.u) : limited_slope<LIM>(m.v, c.v, p.v);
-    s[2] = XDIR ? limited_slope<LIM>(m.v, c.v, p.v) : limited_slope<LIM>(m.u, c.u, p.u);
-    s[3] = limited_slope<LIM>(m.p, c.p, p.p);
-}
-
 // One face of computeFluxesKernel (x: src/solver.cu:1502-1598, y: :1601-1682)
 // from the two cells a | b and their limited slopes sa, sb (cell_slopes):
 // MUSCL reconstruction of (rho, u, v, p), clamps, Riemann flux and the
@@ -279,16 +269,6 @@ __device__ __forceinline__ void face_flux_sl(bool valid, bool near_wall, const P
         out[3] = 0.0f;
         out[4] = 0.0f;
     }
-}
-
-// One face from the four stencil cells m1, a | b, p2.
-template <bool XDIR, int SCHEME, int LIM>
-__device__ __forceinline__ void face_flux(bool valid, bool near_wall, const Prim &m1, const Prim &a, const Prim &b,
-                                          const Prim &p2, float out[5]) {
-    float sa[4], sb[4];
-    cell_slopes<XDIR, LIM>(m1, a, b, sa);
-    cell_slopes<XDIR, LIM>(a, b, p2, sb);
-    face_flux_sl<XDIR, SCHEME>(valid, near_wall, a, sa, b, sb, out);
 }
 
 // updateKernel body for a non-wall cell (src/solver.cu:1736-1875).

@@ -15,8 +15,9 @@
 //
 // The arithmetic is face_flux_sl + hllc_flux (fvm_math.cuh; reference
 // computeFluxesKernel, src/solver.cu:1502-1598 / :1601-1682, and its HLLC,
-// :1112-1223 / :1315-1430) with explicit fused multiply-adds, so results can
-// differ from the scalar form in the last bits.
+// :1112-1223 / :1315-1430) with explicit fused multiply-adds and one
+// approximate reciprocal per shared divisor, so results can differ from the
+// scalar form in the last bits.
 #pragma once
 #include "fvm_math.cuh"
 
@@ -160,7 +161,22 @@ __device__ __forceinline__ void face_pair_core(bool valid0, bool near0, bool val
     const f2 uf = p_add(nL, nR);  // sign of 0.5 (unL + unR)
     const f2 F4 = p_sel(uf.x >= 0.0f, uf.y >= 0.0f, p_mul(eL, nL), p_mul(eR, nR));
     const f2 Fx = XDIR ? Fn : Ft, Fy = XDIR ? Ft : Fn;
-    // wall faces: no mass/energy flux, normal momentum flux = pressure of the left/bottom cell
+    // wall faces: no mass/energy flux, normal momentum flux = pressure of the left/bottom cell.
+    // Most warps have no wall face at all; they skip the per-face selects.
+    // (Every caller evaluates its faces with the whole warp converged.)
+    if (__all_sync(0xffffffffu, valid0 && valid1)) {
+        f0[0] = F0.x;
+        f0[1] = Fx.x;
+        f0[2] = Fy.x;
+        f0[3] = F3.x;
+        f0[4] = F4.x;
+        f1[0] = F0.y;
+        f1[1] = Fx.y;
+        f1[2] = Fy.y;
+        f1[3] = F3.y;
+        f1[4] = F4.y;
+        return;
+    }
     f0[0] = valid0 ? F0.x : 0.0f;
     f0[1] = valid0 ? Fx.x : (XDIR ? a.p.x : 0.0f);
     f0[2] = valid0 ? Fy.x : (XDIR ? 0.0f : a.p.x);
@@ -194,28 +210,6 @@ __device__ __forceinline__ void face_pair_x_sl(bool valid0, bool near0, bool val
                                    Prim{b.rho.y, b.u.y, b.v.y, b.p.y}, sb1, f1);
         return;
     }
-    face_pair_core<true>(valid0, near0, valid1, near1, a, sa, b, sb, f0, f1);
-}
-
-// x-faces of rows r (lane .x -> f0) and r+1 (lane .y -> f1) between cells
-// a | b, stencil m1, a, b, p2.
-template <int SCHEME, int LIM>
-__device__ __forceinline__ void face_pair_x(bool valid0, bool near0, bool valid1, bool near1, const PairPrim &m1,
-                                            const PairPrim &a, const PairPrim &b, const PairPrim &p2, float f0[5],
-                                            float f1[5]) {
-    if (SCHEME != 0) {  // AUSM+: per lane through the scalar path
-        face_flux<true, SCHEME, LIM>(valid0, near0, Prim{m1.rho.x, m1.u.x, m1.v.x, m1.p.x},
-                                     Prim{a.rho.x, a.u.x, a.v.x, a.p.x}, Prim{b.rho.x, b.u.x, b.v.x, b.p.x},
-                                     Prim{p2.rho.x, p2.u.x, p2.v.x, p2.p.x}, f0);
-        face_flux<true, SCHEME, LIM>(valid1, near1, Prim{m1.rho.y, m1.u.y, m1.v.y, m1.p.y},
-                                     Prim{a.rho.y, a.u.y, a.v.y, a.p.y}, Prim{b.rho.y, b.u.y, b.v.y, b.p.y},
-                                     Prim{p2.rho.y, p2.u.y, p2.v.y, p2.p.y}, f1);
-        return;
-    }
-    const PairSl sa{p_slope<LIM>(m1.rho, a.rho, b.rho), p_slope<LIM>(m1.u, a.u, b.u), p_slope<LIM>(m1.v, a.v, b.v),
-                    p_slope<LIM>(m1.p, a.p, b.p)};
-    const PairSl sb{p_slope<LIM>(a.rho, b.rho, p2.rho), p_slope<LIM>(a.u, b.u, p2.u), p_slope<LIM>(a.v, b.v, p2.v),
-                    p_slope<LIM>(a.p, b.p, p2.p)};
     face_pair_core<true>(valid0, near0, valid1, near1, a, sa, b, sb, f0, f1);
 }
 

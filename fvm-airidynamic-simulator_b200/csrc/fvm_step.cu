@@ -457,10 +457,11 @@ struct ViscLayout {
     static constexpr size_t raw_bytes = (size_t)K * SLOT * 4;
     static constexpr size_t p_off = raw_off + raw_bytes;
     static constexpr size_t p_bytes = (size_t)PP * 2 * NT * 16;
-    // stress / heat flux per (row, column): {txx, tyy, txy, qx} in a float4
-    // plane, qy in a float plane
+    // stress / heat flux, one float plane per component: the divergence reads
+    // only the components it uses (3 of 5 per neighbour), which keeps the
+    // shared-memory bytes per cell below those of vector loads
     static constexpr size_t t_off = p_off + p_bytes;
-    static constexpr size_t t_bytes = (size_t)TP * 2 * NT * (16 + 4);
+    static constexpr size_t t_bytes = (size_t)TP * 2 * 5 * NT * 4;
     static constexpr size_t m_off = t_off + t_bytes;
     static constexpr size_t m_bytes = (size_t)PP * 2 * NT;
     static constexpr size_t bar_off = (m_off + m_bytes + 15) & ~(size_t)15;
@@ -490,9 +491,8 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
     constexpr int KP = L::KP;
     static_assert(L::PP == 3 && L::TP == 2 && KP >= 2, "ring sizes");
     float *raw = reinterpret_cast<float *>(smem + L::raw_off);
-    float4 *P = reinterpret_cast<float4 *>(smem + L::p_off);     // {u, v, T, mu}
-    float4 *T4 = reinterpret_cast<float4 *>(smem + L::t_off);    // {txx, tyy, txy, qx}, [row][column]
-    float *T1 = reinterpret_cast<float *>(T4 + L::TP * 2 * NT);  // qy, [row][column]
+    float4 *P = reinterpret_cast<float4 *>(smem + L::p_off);  // {u, v, T, mu}
+    float *Tq = reinterpret_cast<float *>(smem + L::t_off);   // {txx, tyy, txy, qx, qy}
     uint8_t *M = smem + L::m_off;
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bar_off);
 
@@ -614,8 +614,9 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
             }
 #pragma unroll
             for (int h = 0; h < 2; h++) {
-                T4[(tc0 + h) * NT + t] = make_float4(out[h][0], out[h][1], out[h][2], out[h][3]);
-                T1[(tc0 + h) * NT + t] = out[h][4];
+                float *Ts = Tq + (tc0 + h) * 5 * NT + t;
+#pragma unroll
+                for (int k = 0; k < 5; k++) Ts[k * NT] = out[h][k];
             }
         }
         // south neighbour of row r-2 (row r-3, pair q-2): read before its slot is reused
@@ -633,15 +634,20 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
                 const int prow = pc1 + h;
                 store[h] = col_ok && urow >= j0 && urow < j1;
                 ctype[h] = mb_type(M[prow * NT + tp]);
-                // stress rows urow-1, urow, urow+1 (qy only of the north and south rows)
+                // stress rows urow-1, urow, urow+1
                 const int tS = h ? tc1 + 1 : tc1, tC0 = h ? tc0 : tc1 + 1, tN = h ? tc0 + 1 : tc0;
-                const float4 C4 = T4[tC0 * NT + tp], E4 = T4[tC0 * NT + tp + 1], W4 = T4[tC0 * NT + tp - 1];
-                const float4 N4 = T4[tN * NT + tp], S4 = T4[tS * NT + tp];
-                const float tC[5] = {C4.x, C4.y, C4.z, C4.w, 0.0f};
-                const float tE[5] = {E4.x, E4.y, E4.z, E4.w, 0.0f};
-                const float tW[5] = {W4.x, W4.y, W4.z, W4.w, 0.0f};
-                const float tNn[5] = {N4.x, N4.y, N4.z, N4.w, T1[tN * NT + tp]};
-                const float tSs[5] = {S4.x, S4.y, S4.z, S4.w, T1[tS * NT + tp]};
+                const float *T0 = Tq + tC0 * 5 * NT + tp;
+                const float *TN = Tq + tN * 5 * NT + tp;
+                const float *TS = Tq + tS * 5 * NT + tp;
+                float tC[5], tE[5], tW[5], tNn[5], tSs[5];
+#pragma unroll
+                for (int k = 0; k < 5; k++) {
+                    tC[k] = T0[k * NT];
+                    tE[k] = T0[k * NT + 1];
+                    tW[k] = T0[k * NT - 1];
+                    tNn[k] = TN[k * NT];
+                    tSs[k] = TS[k * NT];
+                }
                 const float4 E = P[prow * NT + tp + 1], Wc = P[prow * NT + tp - 1];
                 const float4 N = P[(h ? pc0 : pc1 + 1) * NT + tp];
                 const float4 S = h ? P[pc1 * NT + tp] : S0;

@@ -58,8 +58,8 @@ STEP_BYTES_NS = 184
 # DRAM bytes (read + write) per launch measured by ncu on the 4096x2048 case
 # and scaled by the cell count to 8192x4096 (profiles/marching_kernels_*.md).
 MEASURED_TRAFFIC = {
-    ("ns_hypersonic_cone", 8192, 4096): {"stage1": 1255984128, "stage2": 1973966848,
-                                         "viscous_pre": 1235775488, "viscous_post": 1231261696},
+    ("ns_hypersonic_cone", 8192, 4096): {"stage1": 1252007936, "stage2": 1939415064,
+                                         "viscous_pre": 1235017728, "viscous_post": 1229801472},
 }
 
 
@@ -714,8 +714,8 @@ def main():
         # time step read back at the end of the previous frame, the Mach
         # field into a device buffer (the display buffer), maximum
         # temperature and Mach number to the host at most every 0.25 s (the
-        # first frame included), the next time step queued and read back
-        # (which waits for the frame's work)
+        # first frame included), the next time step queued, the stream
+        # synchronized, the time step read back
         import ctypes as C
         lib = s.lib
         e_fixed = abi.Ext.from_buffer_copy(ext)
@@ -736,6 +736,7 @@ def main():
                 stats_reads[0] += 1
                 stats_reads[1] = now
             fvm_b200._check(lib.fvm_queue_dt(s.h, C.byref(s.params)))
+            fvm_b200._check(lib.fvm_synchronize(s.h))  # the app's cudaDeviceSynchronize
             fvm_b200._check(lib.fvm_read_dt(s.h, C.byref(s.params), C.byref(dt_c)))
 
         fvm_b200._check(lib.fvm_compute_dt(s.h, C.byref(s.params), C.byref(dt_c)))
@@ -821,7 +822,7 @@ def main():
                     "ms_per_frame": app_max / args.steps * 1e3,
                     "protocol": "reference app frame loop, one step per frame: fvm_steps(1) with the host's dt "
                                 "(4 B in), Mach field into a device buffer, max T and max Mach to host every "
-                                "0.25 s, fvm_queue_dt + fvm_read_dt (dt to host, waits for the frame)"},
+                                "0.25 s, fvm_queue_dt + fvm_synchronize + fvm_read_dt (dt to host)"},
             "e2e_state_roundtrip": {"value": e2e_value, "unit": "cell-updates/s", "steps_per_roundtrip": args.steps,
                                     "h2d_bytes_per_step": cells * 20 / args.steps,
                                     "d2h_bytes_per_step": cells * 20 / args.steps,

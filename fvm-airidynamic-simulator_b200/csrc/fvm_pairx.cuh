@@ -161,22 +161,7 @@ __device__ __forceinline__ void face_pair_core(bool valid0, bool near0, bool val
     const f2 uf = p_add(nL, nR);  // sign of 0.5 (unL + unR)
     const f2 F4 = p_sel(uf.x >= 0.0f, uf.y >= 0.0f, p_mul(eL, nL), p_mul(eR, nR));
     const f2 Fx = XDIR ? Fn : Ft, Fy = XDIR ? Ft : Fn;
-    // wall faces: no mass/energy flux, normal momentum flux = pressure of the left/bottom cell.
-    // Most warps have no wall face at all; they skip the per-face selects.
-    // (Every caller evaluates its faces with the whole warp converged.)
-    if (__all_sync(0xffffffffu, valid0 && valid1)) {
-        f0[0] = F0.x;
-        f0[1] = Fx.x;
-        f0[2] = Fy.x;
-        f0[3] = F3.x;
-        f0[4] = F4.x;
-        f1[0] = F0.y;
-        f1[1] = Fx.y;
-        f1[2] = Fy.y;
-        f1[3] = F3.y;
-        f1[4] = F4.y;
-        return;
-    }
+    // wall faces: no mass/energy flux, normal momentum flux = pressure of the left/bottom cell
     f0[0] = valid0 ? F0.x : 0.0f;
     f0[1] = valid0 ? Fx.x : (XDIR ? a.p.x : 0.0f);
     f0[2] = valid0 ? Fy.x : (XDIR ? 0.0f : a.p.x);

@@ -147,7 +147,10 @@ int fvm_step(fvm_handle *h, fvm_sim_params *p);
 int fvm_steps(fvm_handle *h, fvm_sim_params *p, int n);
 /* CFDSolver::computeStableTimeStep (src/solver.cu:3273-3278). */
 int fvm_compute_dt(fvm_handle *h, const fvm_sim_params *p, float *dt_out);
-/* CFDSolver::queueTimeStepComputation / readTimeStepResult (src/solver.cu:3206-3265). */
+/* CFDSolver::queueTimeStepComputation / readTimeStepResult (src/solver.cu:3206-3265).
+ * fvm_queue_dt queues the reduction and its copy to host memory and returns;
+ * fvm_read_dt reads that copy without waiting, so, as with the reference,
+ * the stream must have been synchronized in between (fvm_synchronize). */
 int fvm_queue_dt(fvm_handle *h, const fvm_sim_params *p);
 int fvm_read_dt(fvm_handle *h, const fvm_sim_params *p, float *dt_out);
 /* Block until this handle's stream is idle; reports a device error word. */

@@ -335,6 +335,8 @@ def bench_serving(lams=(10.0, 100.0, 1000.0), n_req=48, chunk=64, budget=150 * 1
         reqs = serving_requests(n_req, lam)
         srv = fvm_b200.Server(ext, budget_bytes=budget, chunk_steps=chunk)
         import threading
+        clk_srv = ClockSampler(torch.cuda.current_device())
+        clk_srv.start()
         t_start = time.perf_counter()
 
         def client():
@@ -351,11 +353,15 @@ def bench_serving(lams=(10.0, 100.0, 1000.0), n_req=48, chunk=64, budget=150 * 1
         res = [r for r, _ in srv.poll(cap=n_req)]
         st = srv.stats()
         srv.close()
+        clocks_served = clk_srv.stop()
         ok = [r for r in res if r.status == 0]
         work = sum(r.nx * r.ny * r.steps for r in ok)
         span = max(r.done_s for r in res) - min(r.submit_s for r in res)
         lat = sorted(r.done_s - r.submit_s for r in ok)
+        clk_solo = ClockSampler(torch.cuda.current_device())
+        clk_solo.start()
         solo_lat, solo_span, solo_work = one_at_a_time(torch, fvm_b200, reqs, ext, stream)
+        clocks_solo = clk_solo.stop()
         # every request at its class's single-solve rate: the work-weighted
         # single-solve rate, the one-at-a-time rate without set-up or idle time
         solo_model_s = sum(p.nx * p.ny * n / class_rate[(p.nx, bool(p.enable_viscosity))] for _, p, n in reqs)
@@ -367,7 +373,9 @@ def bench_serving(lams=(10.0, 100.0, 1000.0), n_req=48, chunk=64, budget=150 * 1
             "device_busy_frac": st.busy_s / span,
             "one_at_a_time": {"value": solo_work / solo_span, "unit": "cell-updates/s",
                               "completion_s_p50": q(solo_lat, 0.5), "completion_s_p99": q(solo_lat, 0.99),
-                              "measured": "same arrivals, one single-solve handle at a time, FIFO, wall clock"},
+                              "measured": "same arrivals, one single-solve handle at a time, FIFO, wall clock",
+                              "clocks": clocks_solo},
+            "clocks": clocks_served,
             "speedup_vs_one_at_a_time": (work / span) / (solo_work / solo_span),
             "single_solve_rate_work_weighted": solo_work / solo_model_s,
             "batched_steps": st.batched_steps,

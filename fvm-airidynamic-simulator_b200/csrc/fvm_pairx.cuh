@@ -40,6 +40,8 @@ __device__ __forceinline__ f2 p_sqrt(f2 a) { return mk2(sqrtf(a.x), sqrtf(a.y));
 __device__ __forceinline__ f2 p_div(f2 a, f2 b) { return mk2(__fdividef(a.x, b.x), __fdividef(a.y, b.y)); }
 // per-lane approximate reciprocal, shared by quotients with one divisor
 __device__ __forceinline__ f2 p_rcp(f2 a) { return mk2(rcp_approx(a.x), rcp_approx(a.y)); }
+// per-lane approximate reciprocal square root
+__device__ __forceinline__ f2 p_rsqrt(f2 a) { return mk2(rsqrtf(a.x), rsqrtf(a.y)); }
 __device__ __forceinline__ f2 p_sel(bool cx, bool cy, f2 a, f2 b) { return mk2(cx ? a.x : b.x, cy ? a.y : b.y); }
 
 // Limited slope per lane (as limited_slope).
@@ -110,10 +112,13 @@ __device__ __forceinline__ void face_pair_core(bool valid0, bool near0, bool val
     // ---- HLLC with Roe-averaged Davis wave speeds; quotients that share a
     // divisor (1/rho of each side, the Roe weight sum, the star-state
     // denominator) multiply by one reciprocal
-    const f2 irL = p_rcp(rL), irR = p_rcp(rR);
+    // one reciprocal square root per side gives sqrt(rho) = rho / sqrt(rho)
+    // and 1/rho = (1/sqrt(rho))^2
+    const f2 rqL = p_rsqrt(rL), rqR = p_rsqrt(rR);
+    const f2 sqL = p_mul(rL, rqL), sqR = p_mul(rR, rqR);
+    const f2 irL = p_mul(rqL, rqL), irR = p_mul(rqR, rqR);
     const f2 cL = p_sqrt(p_mul(p_mul(splat(GAMMA), pL), irL));
     const f2 cR = p_sqrt(p_mul(p_mul(splat(GAMMA), pR), irR));
-    const f2 sqL = p_sqrt(rL), sqR = p_sqrt(rR);
     const f2 iden = p_rcp(p_add(p_add(sqL, sqR), splat(1e-10f)));
     const f2 un_roe = p_mul(p_fma(sqL, nL, p_mul(sqR, nR)), iden);
     const f2 ut_roe = p_mul(p_fma(sqL, tL, p_mul(sqR, tR)), iden);

@@ -492,10 +492,6 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
     static_assert(L::PP == 3 && L::TP == 2 && KP >= 2, "ring sizes");
     float *raw = reinterpret_cast<float *>(smem + L::raw_off);
     float4 *P = reinterpret_cast<float4 *>(smem + L::p_off);  // {u, v, T, mu}
-    // the same ring read as {u, v} pairs or single floats, where a phase uses
-    // only part of an entry (fewer shared-memory bytes per load)
-    const float2 *Puv = reinterpret_cast<const float2 *>(P);  // entry e: Puv[2e] = {u, v}
-    const float *Pf = reinterpret_cast<const float *>(P);     // entry e: Pf[4e + 3] = mu
     float *Tq = reinterpret_cast<float *>(smem + L::t_off);   // {txx, tyy, txy, qx, qy}
     uint8_t *M = smem + L::m_off;
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bar_off);
@@ -607,10 +603,9 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
                 const int rowS = j_lo ? rowC : (h ? pc1 + 1 : pc1);
                 const int rowN = j_hi ? rowC : (h ? pc0 + 1 : pc0);
                 const float fy = (j_lo || j_hi) ? va.inv_dy : va.inv_2dy;
-                const float muC = Pf[4 * (rowC * NT + t) + 3];
-                const float4 E = P[rowC * NT + tE], Wc = P[rowC * NT + tW];
+                const float4 C = P[rowC * NT + t], E = P[rowC * NT + tE], Wc = P[rowC * NT + tW];
                 const float4 N = P[rowN * NT + t], S = P[rowS * NT + t];
-                stress_heat_sel(muC, E.x, Wc.x, N.x, S.x, E.y, Wc.y, N.y, S.y, E.z, Wc.z, N.z, S.z, fx, fy, va,
+                stress_heat_sel(C.w, E.x, Wc.x, N.x, S.x, E.y, Wc.y, N.y, S.y, E.z, Wc.z, N.z, S.z, fx, fy, va,
                                 out[h]);
                 const bool live = stress_col_in && trow >= 0 && trow < ny &&
                                   mb_type(M[rowC * NT + t]) != CT_SOLID;
@@ -625,7 +620,7 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
             }
         }
         // south neighbour of row r-2 (row r-3, pair q-2): read before its slot is reused
-        const float2 S0 = Puv[2 * ((pc2 + 1) * NT + tp)];
+        const float4 S0 = P[(pc2 + 1) * NT + tp];
         __syncthreads();
         // ---- phase 3: viscous update of rows r-2, r-1 at column ic (rows
         // of this tile from step 2 on)
@@ -653,11 +648,12 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
                     tNn[k] = TN[k * NT];
                     tSs[k] = TS[k * NT];
                 }
-                const float2 E = Puv[2 * (prow * NT + tp + 1)], Wc = Puv[2 * (prow * NT + tp - 1)];
-                const float2 N = Puv[2 * ((h ? pc0 : pc1 + 1) * NT + tp)];
-                const float2 S = h ? Puv[2 * (pc1 * NT + tp)] : S0;
+                const float4 E = P[prow * NT + tp + 1], Wc = P[prow * NT + tp - 1];
+                const float4 N = P[(h ? pc0 : pc1 + 1) * NT + tp];
+                const float4 S = h ? P[pc1 * NT + tp] : S0;
                 float rhs[4];
-                viscous_rhs_xy(tC, tE, tW, tNn, tSs, E, Wc, N, S, va, rhs);
+                viscous_rhs_xy(tC, tE, tW, tNn, tSs, mk2(E.x, E.y), mk2(Wc.x, Wc.y), mk2(N.x, N.y), mk2(S.x, S.y), va,
+                               rhs);
                 const bool upd = ctype[h] == CT_FLUID && interior_x && urow > 0 && urow < ny - 1;
                 U[h][0] = Uprev[h][0];
 #pragma unroll
@@ -681,7 +677,7 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
                     lmax_speed = counted ? fmaxf(lmax_speed, ws) : lmax_speed;
                     nbad += counted ? nonfinite5(U[h]) : 0u;
                     if (a.cfl == 2) {
-                        const float mu = (ctype[h] == CT_SOLID) ? 0.0f : Pf[4 * ((pc1 + h) * NT + tp) + 3];
+                        const float mu = (ctype[h] == CT_SOLID) ? 0.0f : P[(pc1 + h) * NT + tp].w;
                         const float nu = mu * rcp_approx(U[h][0] + 1e-10f);
                         lmax_nu = counted ? fmaxf(lmax_nu, nu) : lmax_nu;
                     }

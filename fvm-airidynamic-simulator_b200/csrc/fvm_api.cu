@@ -1066,10 +1066,14 @@ extern "C" int fvm_autotune(fvm_handle *h, const fvm_sim_params *p, int steps, f
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     int rc = FVM_OK;
-    const int nts[2] = {128, 256}, rings[2] = {4, 6}, rows[7] = {4, 8, 16, 32, 64, 128, 256};
+    // tile heights between the powers of two let the tuner fill the last
+    // wave of CTAs (e.g. 8192x4096: 64-row tiles are 4.83 waves on 148 SMs)
+    constexpr int kRows = 13;
+    const int nts[2] = {128, 256}, rings[2] = {4, 6},
+              rows[kRows] = {4, 8, 16, 24, 32, 40, 48, 56, 64, 80, 96, 128, 256};
     for (int a1 = 0; a1 < 2 && rc == FVM_OK; a1++)
         for (int a2 = 0; a2 < 2 && rc == FVM_OK; a2++)
-            for (int a3 = 0; a3 < 7 && rc == FVM_OK; a3++) {
+            for (int a3 = 0; a3 < kRows && rc == FVM_OK; a3++) {
                 StageTune cand{nts[a1], rings[a2], rows[a3]};
                 if (rows[a3] > std::max(16, h->g.ny)) continue;
                 h->tune = cand;

@@ -427,6 +427,35 @@ def reference_cuda(grids=((8192, 4096), (1024, 512)), steps=20):
             "rows": rows, "clocks": clocks.stop()}
 
 
+def grid_scaling(torch, fvm_b200, nx=4096, ny=2048, steps=20, settle=20):
+    """The cone workload at another grid size (autotuned launch shape): device
+    time per step and per kernel, to set beside the 8192x4096 figures."""
+    params, ext = abi.workload("ns_hypersonic_cone", nx, ny)
+    ext.dt_policy = abi.DT_RECOMPUTE
+    stream = torch.cuda.Stream()
+    s = fvm_b200.Solver(params, ext)
+    s.set_stream(stream.cuda_stream)
+    with torch.cuda.stream(stream):
+        s.step(settle)
+        s.autotune(steps=4)
+        s.step(5)
+        ev0, ev1 = _events(torch)
+        ev0.record(stream)
+        s.step(steps)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1) / steps
+        s.set_kernel_timing(True)
+        s.step(10)
+        s.synchronize()
+        kt = s.kernel_times()
+        s.set_kernel_timing(False)
+    tune = dict(zip(("threads", "ring", "rows_per_cta"), s.tune()))
+    s.close()
+    return {"grid": f"{nx}x{ny}", "cells": nx * ny, "ms_per_step": ms, "cell_updates_per_s": nx * ny / (ms / 1e3),
+            "kernels": {k: {"launches": v[0], "avg_ms": v[1] / v[0]} for k, v in kt.items()}, "tune": tune}
+
+
 def run_reference_arm(args, params, ext, ws, rank, dist):
     if rank != 0:
         return
@@ -799,7 +828,9 @@ def main():
     s.close()
     extras = {}
     if rank == 0 and ws == 1 and not args.no_extras:
+        import torch
         for name, fn in (("reference_cuda", reference_cuda),
+                         ("scaling_4096x2048", lambda: grid_scaling(torch, fvm_b200)),
                          ("batched", lambda: bench_batched(n_inst=args.instances, steps=10, warmup=args.warmup)),
                          ("serving", lambda: bench_serving(lams=(10.0, 100.0, 1000.0), n_req=args.requests))):
             try:
@@ -825,12 +856,15 @@ def main():
                          "algorithmic_bytes_per_cell": KERNEL_BYTES[dom_name], "peak_kind": peak_kind},
             "kernels": {k: {"launches": v[0], "avg_ms": v[1] / v[0]} for k, v in ktimes.items()},
             "cpu_baseline": cpu,
-            "e2e": {"value": app_value, "unit": "cell-updates/s", "h2d_bytes_per_step": 4,
-                    "d2h_bytes_per_step": 4 + 8 * app_stats_reads / args.steps,
+            # per frame: dt and simulated time to the device as 8 B of kernel
+            # arguments; the 176-byte device-scalar block back by fvm_queue_dt and
+            # again by fvm_synchronize (error word), 4 B per statistic read
+            "e2e": {"value": app_value, "unit": "cell-updates/s", "h2d_bytes_per_step": 8,
+                    "d2h_bytes_per_step": 2 * 176 + 8 * app_stats_reads / args.steps,
                     "ms_per_frame": app_max / args.steps * 1e3,
-                    "protocol": "reference app frame loop, one step per frame: fvm_steps(1) with the host's dt "
-                                "(4 B in), Mach field into a device buffer, max T and max Mach to host every "
-                                "0.25 s, fvm_queue_dt + fvm_synchronize + fvm_read_dt (dt to host)"},
+                    "protocol": "reference app frame loop, one step per frame: fvm_steps(1) with the host's dt, "
+                                "Mach field into a device buffer, max T and max Mach to host every 0.25 s, "
+                                "fvm_queue_dt + fvm_synchronize + fvm_read_dt (dt to host)"},
             "e2e_state_roundtrip": {"value": e2e_value, "unit": "cell-updates/s", "steps_per_roundtrip": args.steps,
                                     "h2d_bytes_per_step": cells * 20 / args.steps,
                                     "d2h_bytes_per_step": cells * 20 / args.steps,

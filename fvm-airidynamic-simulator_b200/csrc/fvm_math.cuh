@@ -608,6 +608,31 @@ __device__ __forceinline__ void stress_heat_sel(float mu_val, float uE, float uW
     out[3] = -k_val * ((TE - TW) * fx);
     out[4] = -k_val * ((TN - TS) * fy);
 }
+// stress_heat_sel plus what the divergence of the viscous update needs from
+// this cell: the work terms u tau_xx + v tau_xy and u tau_xy + v tau_yy, and
+// the dissipation Phi = tau_xx du/dx + tau_yy dv/dy + tau_xy (du/dy + dv/dx)
+// (src/solver.cu:2437-2510).  out = {txx, tyy, txy, qx, qy, wx, wy, phi}.
+// In the interior (the only cells the update changes) the velocity
+// gradients are the central differences the reference's update uses.
+__device__ __forceinline__ void stress_heat_work_sel(float mu_val, float uC, float vC, float uE, float uW, float uN,
+                                                     float uS, float vE, float vW, float vN, float vS, float TE,
+                                                     float TW, float TN, float TS, float fx, float fy,
+                                                     const ViscArgs &va, float out[8]) {
+    float k_val = mu_val * va.cp_over_pr;
+    float du_dx = (uE - uW) * fx;
+    float du_dy = (uN - uS) * fy;
+    float dv_dx = (vE - vW) * fx;
+    float dv_dy = (vN - vS) * fy;
+    float div_v = du_dx + dv_dy;
+    out[0] = mu_val * (2.0f * du_dx - (2.0f / 3.0f) * div_v);
+    out[1] = mu_val * (2.0f * dv_dy - (2.0f / 3.0f) * div_v);
+    out[2] = mu_val * (du_dy + dv_dx);
+    out[3] = -k_val * ((TE - TW) * fx);
+    out[4] = -k_val * ((TN - TS) * fy);
+    out[5] = uC * out[0] + vC * out[2];
+    out[6] = uC * out[2] + vC * out[1];
+    out[7] = out[0] * du_dx + out[1] * dv_dy + out[2] * (du_dy + dv_dx);
+}
 __device__ __forceinline__ void stress_heat(float uC, float vC, float TC, float uE, float uW, float uN, float uS,
                                             float vE, float vW, float vN, float vS, float TE, float TW, float TN,
                                             float TS, bool i_lo, bool i_hi, bool j_lo, bool j_hi,

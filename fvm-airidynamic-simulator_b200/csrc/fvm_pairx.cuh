@@ -236,31 +236,29 @@ __device__ __forceinline__ void face_pair_y(bool valid0, bool near0, bool valid1
 // Divergence terms of the viscous half step for one interior fluid cell
 // (src/solver.cu:2437-2510): rhs = {d(tau_xx)/dx + d(tau_xy)/dy,
 // d(tau_xy)/dx + d(tau_yy)/dy, -div q + div(tau . v), -div q + Phi}, central
-// differences, with the x and y parts of each derivative pair in one FP32x2
-// lane pair: (du/dx, dv/dx),
-// (du/dy, dv/dy), (dtau_xx/dx, dtau_xy/dx), (dtau_xy/dy, dtau_yy/dy),
-// (dqx/dx, dqy/dy), (dwork/dx, dwork/dy).  vE..vS are the neighbours'
-// (u, v), already a register pair in the primitive ring's {u, v, T, mu}
-// entries; t*: {txx, tyy, txy, qx, qy} at C/E/W/N/S.  Each lane performs the
-// scalar form's operations in the same order.
-__device__ __forceinline__ void viscous_rhs_xy(const float tC[5], const float tE[5], const float tW[5],
-                                               const float tN[5], const float tS[5], f2 vE, f2 vW, f2 vN, f2 vS,
-                                               const ViscArgs &va, float rhs[4]) {
+// differences of the per-cell quantities stress_heat_work_sel produced, with
+// the x and y parts of each derivative pair in one FP32x2 lane pair:
+// (dtau_xx/dx, dtau_xy/dx), (dtau_xy/dy, dtau_yy/dy), (dqx/dx, dqy/dy),
+// (dwork_x/dx, dwork_y/dy).  {txx, txy, qx, wx} of the east / west
+// neighbours, {tyy, txy, qy, wy} of the north / south ones, Phi of the cell.
+struct ViscX {
+    float txx, txy, qx, wx;
+};
+struct ViscY {
+    float tyy, txy, qy, wy;
+};
+__device__ __forceinline__ void viscous_rhs_w(const ViscX &E, const ViscX &W, const ViscY &N, const ViscY &S, float phi,
+                                              const ViscArgs &va, float rhs[4]) {
     const f2 i2x = splat(va.inv_2dx), i2y = splat(va.inv_2dy), i2xy = mk2(va.inv_2dx, va.inv_2dy);
-    const f2 dvx = p_mul(p_sub(vE, vW), i2x);  // (du_dx, dv_dx)
-    const f2 dvy = p_mul(p_sub(vN, vS), i2y);  // (du_dy, dv_dy)
-    const f2 dtx = p_mul(p_sub(mk2(tE[0], tE[2]), mk2(tW[0], tW[2])), i2x);  // (dtau_xx_dx, dtau_xy_dx)
-    const f2 dty = p_mul(p_sub(mk2(tN[2], tN[1]), mk2(tS[2], tS[1])), i2y);  // (dtau_xy_dy, dtau_yy_dy)
-    const f2 dq = p_mul(p_sub(mk2(tE[3], tN[4]), mk2(tW[3], tS[4])), i2xy);  // (dqx_dx, dqy_dy)
-    const float Phi = tC[0] * dvx.x + tC[1] * dvy.y + tC[2] * (dvy.x + dvx.y);
-    const float wxp = vE.x * tE[0] + vE.y * tE[2], wxm = vW.x * tW[0] + vW.y * tW[2];
-    const float wyp = vN.x * tN[2] + vN.y * tN[1], wym = vS.x * tS[2] + vS.y * tS[1];
-    const f2 dw = p_mul(p_sub(mk2(wxp, wyp), mk2(wxm, wym)), i2xy);  // (dwork_dx, dwork_dy)
+    const f2 dtx = p_mul(p_sub(mk2(E.txx, E.txy), mk2(W.txx, W.txy)), i2x);  // (dtau_xx_dx, dtau_xy_dx)
+    const f2 dty = p_mul(p_sub(mk2(N.txy, N.tyy), mk2(S.txy, S.tyy)), i2y);  // (dtau_xy_dy, dtau_yy_dy)
+    const f2 dq = p_mul(p_sub(mk2(E.qx, N.qy), mk2(W.qx, S.qy)), i2xy);      // (dqx_dx, dqy_dy)
+    const f2 dw = p_mul(p_sub(mk2(E.wx, N.wy), mk2(W.wx, S.wy)), i2xy);      // (dwork_dx, dwork_dy)
     const f2 r01 = p_add(dtx, dty);
     rhs[0] = r01.x;
     rhs[1] = r01.y;
     rhs[2] = -dq.x - dq.y + dw.x + dw.y;
-    rhs[3] = -dq.x - dq.y + Phi;
+    rhs[3] = -dq.x - dq.y + phi;
 }
 
 }  // namespace fvm

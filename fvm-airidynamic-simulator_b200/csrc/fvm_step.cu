@@ -450,18 +450,19 @@ struct ViscLayout {
     static constexpr int NB = (NT + 4 + kBox - 1) / kBox;
     static constexpr int BW = NB * kBox;
     static constexpr int KP = K / 2;   // input ring: K rows staged as K/2 row pairs
-    static constexpr int PP = 3;       // primitive / mask ring (row pairs)
+    static constexpr int PP = 2;       // primitive / mask ring (row pairs)
     static constexpr int TP = 2;       // stress / heat-flux ring (row pairs)
+    static constexpr int TQ = 8;       // per cell: txx, tyy, txy, qx, qy, work_x, work_y, Phi
     static constexpr int SLOT = NB * kBoxStride;
     static constexpr size_t raw_off = 0;
     static constexpr size_t raw_bytes = (size_t)K * SLOT * 4;
     static constexpr size_t p_off = raw_off + raw_bytes;
     static constexpr size_t p_bytes = (size_t)PP * 2 * NT * 16;
-    // stress / heat flux, one float plane per component: the divergence reads
-    // only the components it uses (3 of 5 per neighbour), which keeps the
-    // shared-memory bytes per cell below those of vector loads
+    // stress, heat flux, work terms and dissipation, one float plane per
+    // quantity: the divergence reads only the ones it uses (4 of 8 per
+    // neighbour, Phi of the cell itself)
     static constexpr size_t t_off = p_off + p_bytes;
-    static constexpr size_t t_bytes = (size_t)TP * 2 * 5 * NT * 4;
+    static constexpr size_t t_bytes = (size_t)TP * 2 * TQ * NT * 4;
     static constexpr size_t m_off = t_off + t_bytes;
     static constexpr size_t m_bytes = (size_t)PP * 2 * NT;
     static constexpr size_t bar_off = (m_off + m_bytes + 15) & ~(size_t)15;
@@ -478,9 +479,13 @@ struct ViscLayout {
 //            rows r, r+1 of its column for its update one step later, so the
 //            input slot is free after the first barrier and is refilled there
 //   -- barrier --
-//   phase 2  stress and heat flux of rows r-1, r on NT-2 columns
+//   phase 2  stress, heat flux, work terms (u tau_xx + v tau_xy, u tau_xy +
+//            v tau_yy) and dissipation of rows r-1, r on NT-2 columns; the
+//            cell classes (and viscosity) of rows r-2, r-1 into registers
 //   -- barrier --
 //   phase 3  viscous update of rows r-2, r-1 on the W = NT-4 middle columns
+//            from the stress ring alone (the primitive ring's pair q-1 may be
+//            refilled by a faster thread's next phase 1 meanwhile)
 // Both rows of a phase are evaluated in straight-line code (validity applied
 // by selects and predicated stores), so their dependency chains interleave.
 template <int NT, int K>
@@ -489,10 +494,11 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
                                              unsigned &nbad) {
     using L = ViscLayout<NT, K>;
     constexpr int KP = L::KP;
-    static_assert(L::PP == 3 && L::TP == 2 && KP >= 2, "ring sizes");
+    static_assert(L::PP == 2 && L::TP == 2 && KP >= 2, "ring sizes");
+    constexpr int TQ = L::TQ;
     float *raw = reinterpret_cast<float *>(smem + L::raw_off);
     float4 *P = reinterpret_cast<float4 *>(smem + L::p_off);  // {u, v, T, mu}
-    float *Tq = reinterpret_cast<float *>(smem + L::t_off);   // {txx, tyy, txy, qx, qy}
+    float *Tq = reinterpret_cast<float *>(smem + L::t_off);   // TQ planes per row
     uint8_t *M = smem + L::m_off;
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bar_off);
 
@@ -543,9 +549,9 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
     const int tp = min(max(t, 1), NT - 2);  // stencil centre kept inside the rings
 
     int kr = base % KP, par = (base / KP) & 1;
-    int pc0 = 0, pc1 = 4, pc2 = 2;  // P/M rows of row pairs q, q-1, q-2
-    int tc0 = 0, tc1 = 2;           // stress rows of row pairs q (rows r-1, r) and q-1
-    float Uprev[2][5];              // conserved state of rows r-2, r-1 at column ic
+    int pc0 = 0, pc1 = 2;  // P/M rows of row pairs q, q-1
+    int tc0 = 0, tc1 = 2;  // stress rows of row pairs q (rows r-1, r) and q-1
+    float Uprev[2][5];     // conserved state of rows r-2, r-1 at column ic
 #pragma unroll
     for (int h = 0; h < 2; h++)
 #pragma unroll
@@ -588,10 +594,11 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
             issue(issued);
             ++issued;
         }
-        // ---- phase 2: stress and heat flux of rows r-1, r at column ic
-        // (step 0 holds rows j0-3, j0-2, which no update of this tile reads)
+        // ---- phase 2: stress, heat flux, work terms and dissipation of rows
+        // r-1, r at column ic (step 0 holds rows j0-3, j0-2, which no update
+        // of this tile reads)
         if (stress_thread && q > 0) {
-            float out[2][5];
+            float out[2][TQ];
 #pragma unroll
             for (int h = 0; h < 2; h++) {
                 const int trow = r - 1 + h;
@@ -605,55 +612,50 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
                 const float fy = (j_lo || j_hi) ? va.inv_dy : va.inv_2dy;
                 const float4 C = P[rowC * NT + t], E = P[rowC * NT + tE], Wc = P[rowC * NT + tW];
                 const float4 N = P[rowN * NT + t], S = P[rowS * NT + t];
-                stress_heat_sel(C.w, E.x, Wc.x, N.x, S.x, E.y, Wc.y, N.y, S.y, E.z, Wc.z, N.z, S.z, fx, fy, va,
-                                out[h]);
+                stress_heat_work_sel(C.w, C.x, C.y, E.x, Wc.x, N.x, S.x, E.y, Wc.y, N.y, S.y, E.z, Wc.z, N.z, S.z,
+                                     fx, fy, va, out[h]);
                 const bool live = stress_col_in && trow >= 0 && trow < ny &&
                                   mb_type(M[rowC * NT + t]) != CT_SOLID;
 #pragma unroll
-                for (int k = 0; k < 5; k++) out[h][k] = live ? out[h][k] : 0.0f;
+                for (int k = 0; k < TQ; k++) out[h][k] = live ? out[h][k] : 0.0f;
             }
 #pragma unroll
             for (int h = 0; h < 2; h++) {
-                float *Ts = Tq + (tc0 + h) * 5 * NT + t;
+                float *Ts = Tq + (tc0 + h) * TQ * NT + t;
 #pragma unroll
-                for (int k = 0; k < 5; k++) Ts[k * NT] = out[h][k];
+                for (int k = 0; k < TQ; k++) Ts[k * NT] = out[h][k];
             }
         }
-        // south neighbour of row r-2 (row r-3, pair q-2): read before its slot is reused
-        const float4 S0 = P[(pc2 + 1) * NT + tp];
+        // classes and viscosity of rows r-2, r-1 (pair q-1) for phase 3: read
+        // now, because a faster thread's next phase 1 refills that pair's slot
+        uint32_t ctype[2];
+        float mu_c[2];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            ctype[h] = mb_type(M[(pc1 + h) * NT + tp]);
+            mu_c[h] = P[(pc1 + h) * NT + tp].w;
+        }
         __syncthreads();
         // ---- phase 3: viscous update of rows r-2, r-1 at column ic (rows
         // of this tile from step 2 on)
         if (q >= 2) {
             float U[2][5];
-            uint32_t ctype[2];
             bool store[2];
 #pragma unroll
             for (int h = 0; h < 2; h++) {
                 const int urow = r - 2 + h;
-                const int prow = pc1 + h;
                 store[h] = col_ok && urow >= j0 && urow < j1;
-                ctype[h] = mb_type(M[prow * NT + tp]);
                 // stress rows urow-1, urow, urow+1
                 const int tS = h ? tc1 + 1 : tc1, tC0 = h ? tc0 : tc1 + 1, tN = h ? tc0 + 1 : tc0;
-                const float *T0 = Tq + tC0 * 5 * NT + tp;
-                const float *TN = Tq + tN * 5 * NT + tp;
-                const float *TS = Tq + tS * 5 * NT + tp;
-                float tC[5], tE[5], tW[5], tNn[5], tSs[5];
-#pragma unroll
-                for (int k = 0; k < 5; k++) {
-                    tC[k] = T0[k * NT];
-                    tE[k] = T0[k * NT + 1];
-                    tW[k] = T0[k * NT - 1];
-                    tNn[k] = TN[k * NT];
-                    tSs[k] = TS[k * NT];
-                }
-                const float4 E = P[prow * NT + tp + 1], Wc = P[prow * NT + tp - 1];
-                const float4 N = P[(h ? pc0 : pc1 + 1) * NT + tp];
-                const float4 S = h ? P[pc1 * NT + tp] : S0;
+                const float *T0 = Tq + tC0 * TQ * NT + tp;
+                const float *TN = Tq + tN * TQ * NT + tp;
+                const float *TS = Tq + tS * TQ * NT + tp;
+                const ViscX Ex{T0[1], T0[2 * NT + 1], T0[3 * NT + 1], T0[5 * NT + 1]};
+                const ViscX Wx{T0[-1], T0[2 * NT - 1], T0[3 * NT - 1], T0[5 * NT - 1]};
+                const ViscY Ny{TN[NT], TN[2 * NT], TN[4 * NT], TN[6 * NT]};
+                const ViscY Sy{TS[NT], TS[2 * NT], TS[4 * NT], TS[6 * NT]};
                 float rhs[4];
-                viscous_rhs_xy(tC, tE, tW, tNn, tSs, mk2(E.x, E.y), mk2(Wc.x, Wc.y), mk2(N.x, N.y), mk2(S.x, S.y), va,
-                               rhs);
+                viscous_rhs_w(Ex, Wx, Ny, Sy, T0[7 * NT], va, rhs);
                 const bool upd = ctype[h] == CT_FLUID && interior_x && urow > 0 && urow < ny - 1;
                 U[h][0] = Uprev[h][0];
 #pragma unroll
@@ -677,7 +679,7 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
                     lmax_speed = counted ? fmaxf(lmax_speed, ws) : lmax_speed;
                     nbad += counted ? nonfinite5(U[h]) : 0u;
                     if (a.cfl == 2) {
-                        const float mu = (ctype[h] == CT_SOLID) ? 0.0f : P[(pc1 + h) * NT + tp].w;
+                        const float mu = (ctype[h] == CT_SOLID) ? 0.0f : mu_c[h];
                         const float nu = mu * rcp_approx(U[h][0] + 1e-10f);
                         lmax_nu = counted ? fmaxf(lmax_nu, nu) : lmax_nu;
                     }
@@ -698,9 +700,8 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
             for (int k = 0; k < 5; k++) Uprev[h][k] = Unext[h][k];
         kr = ring_next<KP>(kr);
         par ^= (kr == 0) ? 1 : 0;
-        pc2 = pc1;
         pc1 = pc0;
-        pc0 = (pc0 == 4) ? 0 : pc0 + 2;
+        pc0 = 2 - pc0;
         tc1 = tc0;
         tc0 = 2 - tc0;
     }

@@ -458,11 +458,9 @@ struct ViscLayout {
     static constexpr size_t raw_bytes = (size_t)K * SLOT * 4;
     static constexpr size_t p_off = raw_off + raw_bytes;
     static constexpr size_t p_bytes = (size_t)PP * 2 * NT * 16;
-    // stress, heat flux, work terms and dissipation of a row as two float4
-    // planes: X = {txx, txy, qx, work_x} (what the x-derivatives read from the
-    // east / west neighbours), Y = {tyy, qy, work_y, Phi} (what the
-    // y-derivatives read from the north / south ones, plus the cell's own Phi);
-    // txy of a north / south neighbour is one float of its X entry
+    // stress, heat flux, work terms and dissipation, one float plane per
+    // quantity: the divergence reads only the ones it uses (4 of 8 per
+    // neighbour, Phi of the cell itself)
     static constexpr size_t t_off = p_off + p_bytes;
     static constexpr size_t t_bytes = (size_t)TP * 2 * TQ * NT * 4;
     static constexpr size_t m_off = t_off + t_bytes;
@@ -500,7 +498,7 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
     constexpr int TQ = L::TQ;
     float *raw = reinterpret_cast<float *>(smem + L::raw_off);
     float4 *P = reinterpret_cast<float4 *>(smem + L::p_off);  // {u, v, T, mu}
-    float4 *Tq = reinterpret_cast<float4 *>(smem + L::t_off);  // per row slot: X plane, then Y plane
+    float *Tq = reinterpret_cast<float *>(smem + L::t_off);   // TQ planes per row
     uint8_t *M = smem + L::m_off;
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bar_off);
 
@@ -623,9 +621,9 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
             }
 #pragma unroll
             for (int h = 0; h < 2; h++) {
-                float4 *Ts = Tq + (tc0 + h) * 2 * NT + t;
-                Ts[0] = make_float4(out[h][0], out[h][2], out[h][3], out[h][5]);
-                Ts[NT] = make_float4(out[h][1], out[h][4], out[h][6], out[h][7]);
+                float *Ts = Tq + (tc0 + h) * TQ * NT + t;
+#pragma unroll
+                for (int k = 0; k < TQ; k++) Ts[k * NT] = out[h][k];
             }
         }
         // classes and viscosity of rows r-2, r-1 (pair q-1) for phase 3: read
@@ -649,17 +647,15 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
                 store[h] = col_ok && urow >= j0 && urow < j1;
                 // stress rows urow-1, urow, urow+1
                 const int tS = h ? tc1 + 1 : tc1, tC0 = h ? tc0 : tc1 + 1, tN = h ? tc0 + 1 : tc0;
-                const float4 *T0 = Tq + tC0 * 2 * NT + tp;
-                const float4 *TN = Tq + tN * 2 * NT + tp;
-                const float4 *TS = Tq + tS * 2 * NT + tp;
-                const float4 xe = T0[1], xw = T0[-1], yn = TN[NT], ys = TS[NT];
-                const float txy_n = reinterpret_cast<const float *>(TN)[1];
-                const float txy_s = reinterpret_cast<const float *>(TS)[1];
-                const float phi = reinterpret_cast<const float *>(T0 + NT)[3];
-                const ViscX Ex{xe.x, xe.y, xe.z, xe.w}, Wx{xw.x, xw.y, xw.z, xw.w};
-                const ViscY Ny{yn.x, txy_n, yn.y, yn.z}, Sy{ys.x, txy_s, ys.y, ys.z};
+                const float *T0 = Tq + tC0 * TQ * NT + tp;
+                const float *TN = Tq + tN * TQ * NT + tp;
+                const float *TS = Tq + tS * TQ * NT + tp;
+                const ViscX Ex{T0[1], T0[2 * NT + 1], T0[3 * NT + 1], T0[5 * NT + 1]};
+                const ViscX Wx{T0[-1], T0[2 * NT - 1], T0[3 * NT - 1], T0[5 * NT - 1]};
+                const ViscY Ny{TN[NT], TN[2 * NT], TN[4 * NT], TN[6 * NT]};
+                const ViscY Sy{TS[NT], TS[2 * NT], TS[4 * NT], TS[6 * NT]};
                 float rhs[4];
-                viscous_rhs_w(Ex, Wx, Ny, Sy, phi, va, rhs);
+                viscous_rhs_w(Ex, Wx, Ny, Sy, T0[7 * NT], va, rhs);
                 const bool upd = ctype[h] == CT_FLUID && interior_x && urow > 0 && urow < ny - 1;
                 U[h][0] = Uprev[h][0];
 #pragma unroll

@@ -418,7 +418,8 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
 }
 
 // Occupancy target: 6 CTAs of 128 threads per SM (80 registers, no spills;
-// stage 2 with its blend ring takes ~36 KB of shared memory per CTA).
+// ~30 KB of shared memory per CTA for stage 1, ~35 KB for stage 2 with its
+// blend pair).
 template <int NT, int K, int STAGE, int SCHEME, int LIM>
 __global__ void __launch_bounds__(NT, 768 / NT)
     k_stage(const __grid_constant__ CUtensorMap tm_in, const __grid_constant__ CUtensorMap tm_blend,
@@ -717,7 +718,7 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
     return true;
 }
 
-// 6 CTAs of 128 threads per SM (80 registers, no spills; ~34 KB of shared memory each).
+// 6 CTAs of 128 threads per SM (80 registers, no spills; ~36 KB of shared memory each).
 template <int NT, int K>
 __global__ void __launch_bounds__(NT, 768 / NT) k_viscous(const __grid_constant__ CUtensorMap tm_in, const StepArgs a) {
     using L = ViscLayout<NT, K>;

@@ -464,9 +464,7 @@ struct ViscLayout {
     // neighbour, Phi of the cell itself)
     static constexpr size_t t_off = p_off + p_bytes;
     static constexpr size_t t_bytes = (size_t)TP * 2 * TQ * NT * 4;
-    static constexpr size_t m_off = t_off + t_bytes;
-    static constexpr size_t m_bytes = (size_t)PP * 2 * NT;
-    static constexpr size_t bar_off = (m_off + m_bytes + 15) & ~(size_t)15;
+    static constexpr size_t bar_off = (t_off + t_bytes + 15) & ~(size_t)15;
     static constexpr size_t total = bar_off + KP * 8 + 128;  // + alignment slack
     static constexpr uint32_t tx_bytes = 2 * 5 * BW * 4;  // one row pair
 };
@@ -475,14 +473,17 @@ struct ViscLayout {
 // src/solver.cu:2251-2511), out of place, marching two rows per step.
 // Thread t owns column i0-2+t in every phase.  Per step q (incoming rows
 // r = j0-2+2q and r+1):
-//   phase 1  primitives (u, v, T) and Sutherland viscosity + masks of rows
-//            r, r+1 on NT columns; the thread keeps the conserved state of
-//            rows r, r+1 of its column for its update one step later, so the
-//            input slot is free after the first barrier and is refilled there
+//   phase 1  primitives (u, v, T) and Sutherland viscosity of rows r, r+1 on
+//            NT columns into the primitive ring; the thread keeps them, the
+//            cells' mask bytes and the conserved state of its own column in
+//            registers (the stress and the update of that column one and two
+//            steps later read them from there), so the input slot is free
+//            after the first barrier and is refilled there
 //   -- barrier --
 //   phase 2  stress, heat flux, work terms (u tau_xx + v tau_xy, u tau_xy +
-//            v tau_yy) and dissipation of rows r-1, r on NT-2 columns; the
-//            cell classes (and viscosity) of rows r-2, r-1 into registers
+//            v tau_yy) and dissipation of rows r-1, r on NT-2 columns: the
+//            column's own rows from registers, the east / west neighbours
+//            from the primitive ring
 //   -- barrier --
 //   phase 3  viscous update of rows r-2, r-1 on the W = NT-4 middle columns
 //            from the stress ring alone (the primitive ring's pair q-1 may be
@@ -500,7 +501,6 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
     float *raw = reinterpret_cast<float *>(smem + L::raw_off);
     float4 *P = reinterpret_cast<float4 *>(smem + L::p_off);  // {u, v, T, mu}
     float *Tq = reinterpret_cast<float *>(smem + L::t_off);   // TQ planes per row
-    uint8_t *M = smem + L::m_off;
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bar_off);
 
     const GridDesc g = a.g;
@@ -550,13 +550,18 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
     const int tp = min(max(t, 1), NT - 2);  // stencil centre kept inside the rings
 
     int kr = base % KP, par = (base / KP) & 1;
-    int pc0 = 0, pc1 = 2;  // P/M rows of row pairs q, q-1
+    int pc0 = 0, pc1 = 2;  // primitive-ring rows of row pairs q, q-1
     int tc0 = 0, tc1 = 2;  // stress rows of row pairs q (rows r-1, r) and q-1
     float Uprev[2][5];     // conserved state of rows r-2, r-1 at column ic
+    float4 Pprev[2];       // {u, v, T, mu} of rows r-2, r-1 at this thread's column
+    uint32_t mprev[2];     // and their mask bytes
 #pragma unroll
-    for (int h = 0; h < 2; h++)
+    for (int h = 0; h < 2; h++) {
 #pragma unroll
         for (int k = 0; k < 5; k++) Uprev[h][k] = 0.0f;
+        Pprev[h] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        mprev[h] = 0u;
+    }
     bool ok_all = true;
 
     for (int q = 0; q < npairs; q++) {
@@ -565,6 +570,8 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
         const uint32_t nB = __ldg(mcol + (size_t)clampi(r + 3, 0, ny - 1) * g.pitch);
         // ---- phase 1: primitives, viscosity and masks of rows r, r+1
         float Unext[2][5];
+        float4 Pcur[2] = {make_float4(0.0f, 0.0f, 0.0f, 0.0f), make_float4(0.0f, 0.0f, 0.0f, 0.0f)};
+        const uint32_t mcur[2] = {mA, mB};
         bool ok = mbar_wait_bounded(&bars[kr], (uint32_t)par);
         if (ok) {
 #pragma unroll
@@ -574,8 +581,8 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
                 for (int k = 0; k < 5; k++) Unext[h][k] = ring_at<L::NB>(src, k, rc_t);
                 float u, v, p, T;
                 prim_from_cons(Unext[h][0], Unext[h][1], Unext[h][2], Unext[h][3], Unext[h][4], u, v, p, T);
-                P[(pc0 + h) * NT + t] = make_float4(u, v, T, sutherland_mu(T));
-                M[(pc0 + h) * NT + t] = (uint8_t)(h ? mB : mA);
+                Pcur[h] = make_float4(u, v, T, sutherland_mu(T));
+                P[(pc0 + h) * NT + t] = Pcur[h];
             }
         } else {
 #pragma unroll
@@ -608,15 +615,16 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
                 // (north) one and the y-difference is one-sided
                 const bool j_lo = trow == 0, j_hi = trow == ny - 1 && !j_lo;
                 const int rowC = h ? pc0 : pc1 + 1;
-                const int rowS = j_lo ? rowC : (h ? pc1 + 1 : pc1);
-                const int rowN = j_hi ? rowC : (h ? pc0 + 1 : pc0);
                 const float fy = (j_lo || j_hi) ? va.inv_dy : va.inv_2dy;
-                const float4 C = P[rowC * NT + t], E = P[rowC * NT + tE], Wc = P[rowC * NT + tW];
-                const float4 N = P[rowN * NT + t], S = P[rowS * NT + t];
+                // the column's own rows trow-1, trow, trow+1 from registers
+                const float4 C = h ? Pcur[0] : Pprev[1];
+                const float4 N = j_hi ? C : (h ? Pcur[1] : Pcur[0]);
+                const float4 S = j_lo ? C : (h ? Pprev[1] : Pprev[0]);
+                const float4 E = P[rowC * NT + tE], Wc = P[rowC * NT + tW];
                 stress_heat_work_sel(C.w, C.x, C.y, E.x, Wc.x, N.x, S.x, E.y, Wc.y, N.y, S.y, E.z, Wc.z, N.z, S.z,
                                      fx, fy, va, out[h]);
                 const bool live = stress_col_in && trow >= 0 && trow < ny &&
-                                  mb_type(M[rowC * NT + t]) != CT_SOLID;
+                                  mb_type(h ? mcur[0] : mprev[1]) != CT_SOLID;
 #pragma unroll
                 for (int k = 0; k < TQ; k++) out[h][k] = live ? out[h][k] : 0.0f;
             }
@@ -627,14 +635,14 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
                 for (int k = 0; k < TQ; k++) Ts[k * NT] = out[h][k];
             }
         }
-        // classes and viscosity of rows r-2, r-1 (pair q-1) for phase 3: read
-        // now, because a faster thread's next phase 1 refills that pair's slot
+        // classes and viscosity of rows r-2, r-1 for phase 3 (the threads that
+        // store updates have tp == t, so their own column's registers)
         uint32_t ctype[2];
         float mu_c[2];
 #pragma unroll
         for (int h = 0; h < 2; h++) {
-            ctype[h] = mb_type(M[(pc1 + h) * NT + tp]);
-            mu_c[h] = P[(pc1 + h) * NT + tp].w;
+            ctype[h] = mb_type(mprev[h]);
+            mu_c[h] = Pprev[h].w;
         }
         __syncthreads();
         // ---- phase 3: viscous update of rows r-2, r-1 at column ic (rows
@@ -696,9 +704,12 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
             }
         }
 #pragma unroll
-        for (int h = 0; h < 2; h++)
+        for (int h = 0; h < 2; h++) {
 #pragma unroll
             for (int k = 0; k < 5; k++) Uprev[h][k] = Unext[h][k];
+            Pprev[h] = Pcur[h];
+            mprev[h] = mcur[h];
+        }
         kr = ring_next<KP>(kr);
         par ^= (kr == 0) ? 1 : 0;
         pc1 = pc0;

@@ -453,15 +453,15 @@ struct ViscLayout {
     static constexpr int KP = K / 2;   // input ring: K rows staged as K/2 row pairs
     static constexpr int PP = 2;       // primitive / mask ring (row pairs)
     static constexpr int TP = 2;       // stress / heat-flux ring (row pairs)
-    static constexpr int TQ = 8;       // per cell: txx, tyy, txy, qx, qy, work_x, work_y, Phi
+    static constexpr int TQ = 4;       // per cell: txx, txy, qx, work_x (what east / west neighbours read)
     static constexpr int SLOT = NB * kBoxStride;
     static constexpr size_t raw_off = 0;
     static constexpr size_t raw_bytes = (size_t)K * SLOT * 4;
     static constexpr size_t p_off = raw_off + raw_bytes;
     static constexpr size_t p_bytes = (size_t)PP * 2 * NT * 16;
-    // stress, heat flux, work terms and dissipation, one float plane per
-    // quantity: the divergence reads only the ones it uses (4 of 8 per
-    // neighbour, Phi of the cell itself)
+    // the x-derivative operands of the divergence (tau_xx, tau_xy, q_x,
+    // work_x), one float plane each; the y-derivative operands and Phi stay in
+    // the registers of the thread that owns the column
     static constexpr size_t t_off = p_off + p_bytes;
     static constexpr size_t t_bytes = (size_t)TP * 2 * TQ * NT * 4;
     static constexpr size_t bar_off = (t_off + t_bytes + 15) & ~(size_t)15;
@@ -485,9 +485,11 @@ struct ViscLayout {
 //            column's own rows from registers, the east / west neighbours
 //            from the primitive ring
 //   -- barrier --
-//   phase 3  viscous update of rows r-2, r-1 on the W = NT-4 middle columns
-//            from the stress ring alone (the primitive ring's pair q-1 may be
-//            refilled by a faster thread's next phase 1 meanwhile)
+//   phase 3  viscous update of rows r-2, r-1 on the W = NT-4 middle columns:
+//            east / west operands from the stress ring, the column's own
+//            north / south operands and Phi from registers (the primitive
+//            ring's pair q-1 may be refilled by a faster thread's next
+//            phase 1 meanwhile)
 // Both rows of a phase are evaluated in straight-line code (validity applied
 // by selects and predicated stores), so their dependency chains interleave.
 template <int NT, int K>
@@ -555,12 +557,15 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
     float Uprev[2][5];     // conserved state of rows r-2, r-1 at column ic
     float4 Pprev[2];       // {u, v, T, mu} of rows r-2, r-1 at this thread's column
     uint32_t mprev[2];     // and their mask bytes
+    ViscY yprev[2];        // {tyy, -, qy, work_y} of rows r-3, r-2 at this column (txy is in the ring)
+    float phi_prev = 0.0f; // Phi of row r-2 at this column
 #pragma unroll
     for (int h = 0; h < 2; h++) {
 #pragma unroll
         for (int k = 0; k < 5; k++) Uprev[h][k] = 0.0f;
         Pprev[h] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         mprev[h] = 0u;
+        yprev[h] = ViscY{0.0f, 0.0f, 0.0f, 0.0f};
     }
     bool ok_all = true;
 
@@ -605,8 +610,10 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
         // ---- phase 2: stress, heat flux, work terms and dissipation of rows
         // r-1, r at column ic (step 0 holds rows j0-3, j0-2, which no update
         // of this tile reads)
+        ViscY ycur[2] = {ViscY{0.0f, 0.0f, 0.0f, 0.0f}, ViscY{0.0f, 0.0f, 0.0f, 0.0f}};
+        float phi_cur[2] = {0.0f, 0.0f};
         if (stress_thread && q > 0) {
-            float out[2][TQ];
+            float out[2][8];
 #pragma unroll
             for (int h = 0; h < 2; h++) {
                 const int trow = r - 1 + h;
@@ -626,13 +633,18 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
                 const bool live = stress_col_in && trow >= 0 && trow < ny &&
                                   mb_type(h ? mcur[0] : mprev[1]) != CT_SOLID;
 #pragma unroll
-                for (int k = 0; k < TQ; k++) out[h][k] = live ? out[h][k] : 0.0f;
+                for (int k = 0; k < 8; k++) out[h][k] = live ? out[h][k] : 0.0f;
             }
+            // out = {txx, tyy, txy, qx, qy, wx, wy, phi}
 #pragma unroll
             for (int h = 0; h < 2; h++) {
                 float *Ts = Tq + (tc0 + h) * TQ * NT + t;
-#pragma unroll
-                for (int k = 0; k < TQ; k++) Ts[k * NT] = out[h][k];
+                Ts[0] = out[h][0];
+                Ts[NT] = out[h][2];
+                Ts[2 * NT] = out[h][3];
+                Ts[3 * NT] = out[h][5];
+                ycur[h] = ViscY{out[h][1], out[h][2], out[h][4], out[h][6]};
+                phi_cur[h] = out[h][7];
             }
         }
         // classes and viscosity of rows r-2, r-1 for phase 3 (the threads that
@@ -654,17 +666,18 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
             for (int h = 0; h < 2; h++) {
                 const int urow = r - 2 + h;
                 store[h] = col_ok && urow >= j0 && urow < j1;
-                // stress rows urow-1, urow, urow+1
-                const int tS = h ? tc1 + 1 : tc1, tC0 = h ? tc0 : tc1 + 1, tN = h ? tc0 + 1 : tc0;
+                // east / west operands of row urow from the ring; north /
+                // south (rows urow+1, urow-1) and Phi from this column's registers
+                const int tC0 = h ? tc0 : tc1 + 1;
                 const float *T0 = Tq + tC0 * TQ * NT + tp;
-                const float *TN = Tq + tN * TQ * NT + tp;
-                const float *TS = Tq + tS * TQ * NT + tp;
-                const ViscX Ex{T0[1], T0[2 * NT + 1], T0[3 * NT + 1], T0[5 * NT + 1]};
-                const ViscX Wx{T0[-1], T0[2 * NT - 1], T0[3 * NT - 1], T0[5 * NT - 1]};
-                const ViscY Ny{TN[NT], TN[2 * NT], TN[4 * NT], TN[6 * NT]};
-                const ViscY Sy{TS[NT], TS[2 * NT], TS[4 * NT], TS[6 * NT]};
+                const ViscX Ex{T0[1], T0[NT + 1], T0[2 * NT + 1], T0[3 * NT + 1]};
+                const ViscX Wx{T0[-1], T0[NT - 1], T0[2 * NT - 1], T0[3 * NT - 1]};
+                const ViscY &Ny = h ? ycur[1] : ycur[0];
+                // the south row's txy from the ring (row r-3 or r-2, pair slot tc1)
+                const ViscY Sy{h ? yprev[1].tyy : yprev[0].tyy, Tq[(tc1 + h) * TQ * NT + NT + tp],
+                               h ? yprev[1].qy : yprev[0].qy, h ? yprev[1].wy : yprev[0].wy};
                 float rhs[4];
-                viscous_rhs_w(Ex, Wx, Ny, Sy, T0[7 * NT], va, rhs);
+                viscous_rhs_w(Ex, Wx, Ny, Sy, h ? phi_cur[0] : phi_prev, va, rhs);
                 const bool upd = ctype[h] == CT_FLUID && interior_x && urow > 0 && urow < ny - 1;
                 U[h][0] = Uprev[h][0];
 #pragma unroll
@@ -709,7 +722,9 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
             for (int k = 0; k < 5; k++) Uprev[h][k] = Unext[h][k];
             Pprev[h] = Pcur[h];
             mprev[h] = mcur[h];
+            yprev[h] = ViscY{ycur[h].tyy, 0.0f, ycur[h].qy, ycur[h].wy};
         }
+        phi_prev = phi_cur[1];
         kr = ring_next<KP>(kr);
         par ^= (kr == 0) ? 1 : 0;
         pc1 = pc0;
@@ -729,9 +744,12 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
     return true;
 }
 
-// 6 CTAs of 128 threads per SM (80 registers, no spills; ~36 KB of shared memory each).
+// 5 CTAs of 128 threads per SM (96 registers, no spills; ~28 KB of shared
+// memory each): the column's own primitives and stress operands live in
+// registers across steps, which at 80 registers (6 CTAs) spilled and ran
+// 15-20 % slower.
 template <int NT, int K>
-__global__ void __launch_bounds__(NT, 768 / NT) k_viscous(const __grid_constant__ CUtensorMap tm_in, const StepArgs a) {
+__global__ void __launch_bounds__(NT, 640 / NT) k_viscous(const __grid_constant__ CUtensorMap tm_in, const StepArgs a) {
     using L = ViscLayout<NT, K>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned char *smem = aligned_smem(smem_raw);

@@ -157,11 +157,15 @@ __device__ __forceinline__ void face_pair_core(bool valid0, bool near0, bool val
     const f2 rs = p_max(p_mul(rkd, icd), MIN_DENSITY);
     const f2 ps = p_max(p_fma(rkd, p_sub(Ss, nK), pK), MIN_PRESSURE);
     const f2 Es = p_mul(p_sub(p_fma(EK, d, p_mul(ps, Ss)), p_mul(pK, nK)), icd);
+    // star region: F = F_K + S_K (U*_K - U_K); supersonic: F = F_K, written
+    // as F_K + 0 * (U*_K - U_K) (there the wave fan keeps |ds| >= rho c, so
+    // the star quantities are finite and the product is exactly zero)
     const bool st0 = !(supL0 || supR0), st1 = !(supL1 || supR1);
-    const f2 F0 = p_sel(st0, st1, p_fma(SK, p_sub(rs, rK), fK0), fK0);
-    const f2 Fn = p_sel(st0, st1, p_fma(SK, p_sub(p_mul(rs, Ss), fK0), fK1), fK1);
-    const f2 Ft = p_sel(st0, st1, p_fma(SK, p_mul(p_sub(rs, rK), tK), fK2), fK2);
-    const f2 F3 = p_sel(st0, st1, p_fma(SK, p_sub(Es, EK), fK3), fK3);
+    const f2 SKs = p_sel(st0, st1, SK, splat(0.0f));
+    const f2 F0 = p_fma(SKs, p_sub(rs, rK), fK0);
+    const f2 Fn = p_fma(SKs, p_sub(p_mul(rs, Ss), fK0), fK1);
+    const f2 Ft = p_fma(SKs, p_mul(p_sub(rs, rK), tK), fK2);
+    const f2 F3 = p_fma(SKs, p_sub(Es, EK), fK3);
     // upwinded internal-energy flux
     const f2 uf = p_add(nL, nR);  // sign of 0.5 (unL + unR)
     const f2 F4 = p_sel(uf.x >= 0.0f, uf.y >= 0.0f, p_mul(eL, nL), p_mul(eR, nR));

@@ -704,7 +704,11 @@ def main():
         s.step(args.settle)
         if not args.no_autotune:
             s.autotune(steps=4)  # launch shape for this grid class (untimed)
-        s.step(args.warmup)
+        # W warm-up steps as W-1 and 1: the first call captures the two-step
+        # graphs, the second the one-step graphs (both buffer parities each),
+        # so the timed steps replay graphs and capture none
+        s.step(max(args.warmup - 1, 2))
+        s.step(1)
         torch.cuda.synchronize()
 
         # ---- timed region (device-resident): K steps
@@ -790,6 +794,8 @@ def main():
         app_max = max_over_ranks(app_s, dist)
         assert np.isfinite(tmax.value) and np.isfinite(mmax.value) and dt_c.value > 0
         s.set_ext(ext)
+        s.step(3)  # captures the step graphs again (a new policy drops them)
+        torch.cuda.synchronize()
 
         # ---- end to end with the whole state through host memory: upload
         # the state from pinned host buffers, K steps, download the state

@@ -661,6 +661,60 @@ static int finish_steps(fvm_handle *h, fvm_sim_params *p, int n) {
     return FVM_OK;
 }
 
+// Which ping-pong buffer holds U^n (0: the one that held it at the first
+// captured step); the captured pointers depend on it.
+static int state_parity(fvm_handle *h) {
+    if (!h->parity_base) h->parity_base = h->buf[BUF_N];
+    return (h->buf[BUF_N] == h->parity_base) ? 0 : 1;
+}
+
+// Captured graphs of `nsteps` steps (2 or 1) for both buffer parities, built
+// together the first time either is needed (and again after a change of
+// their key), so no later call pays for a capture and an instantiation.  The
+// other parity's graph is captured with the state pointers swapped and
+// restored afterwards; capture launches nothing.
+static int ensure_graphs(fvm_handle *h, int nsteps, cudaGraphExec_t *graphs, unsigned long long *keys) {
+    const int cur = state_parity(h);
+    const unsigned long long key = graph_key(h);
+    for (int par = 0; par < 2; par++) {
+        if (graphs[par] && keys[par] == key) continue;
+        if (graphs[par]) {
+            cudaGraphExecDestroy(graphs[par]);
+            graphs[par] = nullptr;
+        }
+        const bool other = par != cur;
+        if (other) swap_state(h);
+        cudaGraph_t gr;
+        cudaError_t eb = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
+        if (eb != cudaSuccess) {
+            if (other) swap_state(h);
+            CK(eb);
+        }
+        long long before = h->launches;
+        // two steps swap the state twice (also when a step fails to enqueue),
+        // one step not at all: the pointers end as they began
+        int r = enqueue_step(h);
+        if (nsteps == 2) {
+            swap_state(h);
+            if (!r) r = enqueue_step(h);
+            swap_state(h);
+        }
+        cudaError_t ec = cudaStreamEndCapture(h->stream, &gr);
+        h->launches = before;
+        if (other) swap_state(h);
+        if (r) {
+            if (ec == cudaSuccess) cudaGraphDestroy(gr);
+            return r;
+        }
+        CK(ec);
+        cudaError_t ei = cudaGraphInstantiate(&graphs[par], gr, 0);
+        cudaGraphDestroy(gr);
+        CK(ei);
+        keys[par] = key;
+    }
+    return FVM_OK;
+}
+
 extern "C" int fvm_step(fvm_handle *h, fvm_sim_params *p) { return fvm_steps(h, p, 1); }
 
 extern "C" int fvm_steps(fvm_handle *h, fvm_sim_params *p, int n) {
@@ -684,31 +738,8 @@ extern "C" int fvm_steps(fvm_handle *h, fvm_sim_params *p, int n) {
                            h->stream != cudaStreamPerThread && getenv("FVM_NO_GRAPH") == nullptr;
     int done = 0;
     if (use_graph && n >= 2) {
-        // the captured pointers depend on which ping-pong buffer holds U^n
-        if (!h->parity_base) h->parity_base = h->buf[BUF_N];
-        const int par = (h->buf[BUF_N] == h->parity_base) ? 0 : 1;
-        unsigned long long key = graph_key(h);
-        if (h->graph[par] && h->graph_key[par] != key) {
-            cudaGraphExecDestroy(h->graph[par]);
-            h->graph[par] = nullptr;
-        }
-        if (!h->graph[par]) {
-            cudaGraph_t gr;
-            CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-            long long before = h->launches;
-            int r1 = enqueue_step(h);
-            swap_state(h);
-            int r2 = r1 ? r1 : enqueue_step(h);
-            swap_state(h);
-            cudaError_t ec = cudaStreamEndCapture(h->stream, &gr);
-            h->launches = before;
-            if (r1 || r2) return r1 ? r1 : r2;
-            CK(ec);
-            cudaError_t ei = cudaGraphInstantiate(&h->graph[par], gr, 0);
-            cudaGraphDestroy(gr);
-            CK(ei);
-            h->graph_key[par] = key;
-        }
+        const int par = state_parity(h);
+        if (int r = ensure_graphs(h, 2, h->graph, h->graph_key)) return r;
         const int per_step = h->prm.enable_viscosity ? 6 : 4;
         for (; done + 2 <= n; done += 2) {
             CK(cudaGraphLaunch(h->graph[par], h->stream));
@@ -717,27 +748,8 @@ extern "C" int fvm_steps(fvm_handle *h, fvm_sim_params *p, int n) {
     }
     if (use_graph && done < n) {
         // one remaining step: a captured single step for this buffer parity
-        if (!h->parity_base) h->parity_base = h->buf[BUF_N];
-        const int par = (h->buf[BUF_N] == h->parity_base) ? 0 : 1;
-        unsigned long long key = graph_key(h);
-        if (h->graph1[par] && h->graph1_key[par] != key) {
-            cudaGraphExecDestroy(h->graph1[par]);
-            h->graph1[par] = nullptr;
-        }
-        if (!h->graph1[par]) {
-            cudaGraph_t gr;
-            CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-            long long before = h->launches;
-            int r1 = enqueue_step(h);
-            cudaError_t ec = cudaStreamEndCapture(h->stream, &gr);
-            h->launches = before;
-            if (r1) return r1;
-            CK(ec);
-            cudaError_t ei = cudaGraphInstantiate(&h->graph1[par], gr, 0);
-            cudaGraphDestroy(gr);
-            CK(ei);
-            h->graph1_key[par] = key;
-        }
+        const int par = state_parity(h);
+        if (int r = ensure_graphs(h, 1, h->graph1, h->graph1_key)) return r;
         CK(cudaGraphLaunch(h->graph1[par], h->stream));
         h->launches += h->prm.enable_viscosity ? 6 : 4;
         swap_state(h);
@@ -1080,7 +1092,7 @@ extern "C" int fvm_autotune(fvm_handle *h, const fvm_sim_params *p, int steps, f
                 drop_graphs(h);
                 if ((rc = build_maps(h)) != FVM_OK) break;
                 fvm_sim_params w = q;
-                if ((rc = fvm_steps(h, &w, 2)) != FVM_OK) break;  // warm (graph capture)
+                if ((rc = fvm_steps(h, &w, 3)) != FVM_OK) break;  // warm (captures both graph kinds)
                 cudaEventRecord(e0, h->stream);
                 if ((rc = fvm_steps(h, &w, steps)) != FVM_OK) break;
                 cudaEventRecord(e1, h->stream);

@@ -137,18 +137,26 @@ def test_checkpoint_restore_is_bitwise():
 
 
 def test_runs_are_deterministic_and_graph_replay_matches_single_steps():
+    # "mixed" replays graphs of both buffer parities, among them those
+    # captured for the other parity when the first graph was built; "eager"
+    # launches every kernel without a graph (kernel timing on)
     outs = []
-    for mode in ("graph", "graph", "single"):
+    for mode in ("graph", "graph", "single", "mixed", "eager"):
         s, p, e = _solver("ns_karman_re200", 160, 80)
         p.dt = s.compute_dt()
         if mode == "graph":
             s.step(12)
+        elif mode == "mixed":
+            for n in (2, 1, 2, 3, 1, 3):
+                s.step(n)
         else:
+            if mode == "eager":
+                s.set_kernel_timing(True)
             for _ in range(12):
                 s.step(1)
         outs.append(s.fields())
-    assert np.array_equal(outs[0].view(np.uint32), outs[1].view(np.uint32))
-    assert np.array_equal(outs[0].view(np.uint32), outs[2].view(np.uint32))
+    for k in range(1, len(outs)):
+        assert np.array_equal(outs[0].view(np.uint32), outs[k].view(np.uint32)), k
 
 
 def test_compute_dt_matches_oracle():

@@ -271,67 +271,15 @@ __device__ __forceinline__ void face_flux_sl(bool valid, bool near_wall, const P
     }
 }
 
-// updateKernel body for a non-wall cell (src/solver.cu:1736-1875).
-// fR/fL: x-face fluxes at i+1/2 and i-1/2, fT/fB: y-faces at j+1/2, j-1/2.
-// uR, uL, vT, vB: the faces' velocities for the rho_e source (face_velocity of
-// each face, the same value from either side), p_c: primitive p.
+// Step coefficients of the update: dt, 1/dx, 1/dy.
 struct UpdateArgs {
     float dt, inv_dx, inv_dy;
 };
-// Face velocity of the rho_e source term: mass flux over the mean of the two
-// cells' clamped densities (src/solver.cu:1772-1794).
-__device__ __forceinline__ float face_velocity(float mass_flux, float rho_a, float rho_b) {
-    return mass_flux * rcp_approx(0.5f * (fmaxf(rho_a, MIN_DENSITY) + fmaxf(rho_b, MIN_DENSITY)));
-}
-__device__ __forceinline__ void update_cell(const float U[5], const float fR[5], const float fL[5], const float fT[5],
-                                            const float fB[5], float uR, float uL, float vT, float vB, float p_c,
-                                            bool edge_x, bool edge_y, bool interior, const UpdateArgs &a,
-                                            float out[5]) {
-    // U - dt (dF/dx + dF/dy) as U - (dt/dx) dFx - (dt/dy) dFy; the reference
-    // zeroes the flux difference across a domain edge (i = 0 or nx-1 for x,
-    // j = 0 or ny-1 for y), done here by zeroing the coefficient
-    const float dt = a.dt;
-    const float cx = edge_x ? 0.0f : dt * a.inv_dx;
-    const float cy = edge_y ? 0.0f : dt * a.inv_dy;
-    float n[5];
-#pragma unroll
-    for (int k = 0; k < 5; k++) n[k] = U[k] - cx * (fR[k] - fL[k]) - cy * (fT[k] - fB[k]);
-    // rho_e source -p div(v) from the face velocities (interior cells only)
-    if (interior) {
-        float div_v = (uR - uL) * a.inv_dx + (vT - vB) * a.inv_dy;
-        n[4] += dt * (-p_c * div_v);
-    }
-    float new_rho = n[0], new_rho_u = n[1], new_rho_v = n[2], new_E = n[3], new_rho_e = n[4];
-    if (!isfinite(new_rho) || new_rho < MIN_DENSITY) new_rho = fmaxf(U[0], MIN_DENSITY);
-    if (!isfinite(new_rho_u)) new_rho_u = U[1];
-    if (!isfinite(new_rho_v)) new_rho_v = U[2];
-    if (!isfinite(new_E)) new_E = U[3];
-    if (!isfinite(new_rho_e) || new_rho_e < MIN_PRESSURE / (GAMMA - 1.0f)) new_rho_e = U[4];
-    new_rho = fmaxf(new_rho, MIN_DENSITY);
-    const float inv_rho = rcp_approx(new_rho);
-    float u_new = new_rho_u * inv_rho;
-    float v_new = new_rho_v * inv_rho;
-    // |u| > MAX_VEL compared in squares; the square root only when rescaling
-    float q = u_new * u_new + v_new * v_new;
-    if (q > MAX_VEL * MAX_VEL) {
-        float scale = MAX_VEL / sqrtf(q);
-        u_new *= scale;
-        v_new *= scale;
-        new_rho_u = new_rho * u_new;
-        new_rho_v = new_rho * v_new;
-        q = u_new * u_new + v_new * v_new;
-    }
-    float ke = 0.5f * new_rho * q;
-    float e_internal = dual_energy_low(new_rho_e, new_E) ? new_rho_e : (new_E - ke);
-    constexpr float kEmin = R_GAS * MIN_TEMPERATURE / (GAMMA - 1.0f), kEmax = R_GAS * MAX_TEMPERATURE / (GAMMA - 1.0f);
-    e_internal = fmaxf(e_internal, new_rho * kEmin);
-    e_internal = fminf(e_internal, new_rho * kEmax);
-    out[0] = new_rho;
-    out[1] = new_rho_u;
-    out[2] = new_rho_v;
-    out[3] = e_internal + ke;
-    out[4] = e_internal;
-}
+// Bounds of the specific internal energy per unit density in the update's
+// dual-energy resync: R T_min / (gamma - 1) and R T_max / (gamma - 1)
+// (src/solver.cu:1857-1864).
+constexpr float kEminPerRho = R_GAS * MIN_TEMPERATURE / (GAMMA - 1.0f);
+constexpr float kEmaxPerRho = R_GAS * MAX_TEMPERATURE / (GAMMA - 1.0f);
 
 // ------------------------------------------------------ boundary conditions
 // Riemann invariants along a boundary normal (src/solver.cu:680-841): un is

@@ -1,6 +1,6 @@
-// fvm_pairx.cuh -- the faces a stage-kernel thread evaluates per step in
-// packed FP32x2 arithmetic: the two x-faces (same column, rows r and r+1)
-// and the two y-faces (r-2 | r-1) and (r-1 | r).
+// fvm_pairx.cuh -- what a stage-kernel thread evaluates per step, in packed
+// FP32x2 arithmetic: the two x-faces (same column, rows r and r+1), the two
+// y-faces (r-2 | r-1) and (r-1 | r), and the update of rows r-2 and r-1.
 //
 // sm_100 issues two FP32 adds, multiplies or FMAs per instruction
 // (__fadd2_rn / __fmul2_rn / __ffma2_rn) at the same FMA throughput as the
@@ -13,11 +13,13 @@
 // Square roots, reciprocals, min/max and the wave-fan selections stay per
 // lane.
 //
-// The arithmetic is face_flux_sl + hllc_flux (fvm_math.cuh; reference
+// The face arithmetic is face_flux_sl + hllc_flux (fvm_math.cuh; reference
 // computeFluxesKernel, src/solver.cu:1502-1598 / :1601-1682, and its HLLC,
-// :1112-1223 / :1315-1430) with explicit fused multiply-adds and one
-// approximate reciprocal per shared divisor, so results can differ from the
-// scalar form in the last bits.
+// :1112-1223 / :1315-1430), the update that of updateKernel (:1736-1875),
+// with explicit fused multiply-adds and one approximate reciprocal per
+// shared divisor, so results can differ from the reference's in the last
+// bits.  The x-face ring stores each row pair interleaved as well, so the
+// update's flux differences come out of vector loads as register pairs.
 #pragma once
 #include "fvm_math.cuh"
 
@@ -73,14 +75,13 @@ struct PairSl {
     f2 rho, n, t, p;
 };
 
-// Two faces between cells a | b (lane .x -> f0, lane .y -> f1) from the
-// cells' primitives and limited slopes sa, sb (face frame); out = {mass,
-// x-momentum, y-momentum, energy, rho_e}.  valid*: neither side a wall;
-// near*: first order (wall at the outer stencil cells).
+// Two faces between cells a | b (lane .x: face 0, lane .y: face 1) from the
+// cells' primitives and limited slopes sa, sb (face frame); F = {mass,
+// x-momentum, y-momentum, energy, rho_e}, each a lane pair.  valid*: neither
+// side a wall; near*: first order (wall at the outer stencil cells).
 template <bool XDIR>
 __device__ __forceinline__ void face_pair_core(bool valid0, bool near0, bool valid1, bool near1, const PairPrim &a,
-                                               const PairSl &sa, const PairPrim &b, const PairSl &sb, float f0[5],
-                                               float f1[5]) {
+                                               const PairSl &sa, const PairPrim &b, const PairSl &sb, f2 F[5]) {
     const bool fo0 = near0 || a.rho.x < LOW_DENSITY || b.rho.x < LOW_DENSITY;
     const bool fo1 = near1 || a.rho.y < LOW_DENSITY || b.rho.y < LOW_DENSITY;
     const f2 hp = splat(0.5f);
@@ -150,9 +151,11 @@ __device__ __forceinline__ void face_pair_core(bool valid0, bool near0, bool val
     const f2 fK1 = p_fma(fK0, nK, pK);
     const f2 fK2 = XDIR ? p_mul(fK0, tK) : p_mul(p_mul(rK, tK), nK);  // (rho u) v either way
     const f2 fK3 = p_mul(p_add(EK, pK), nK);
+    // |S_K - S*| floored at 1e-10 with its sign (the reference's
+    // `cd >= 0 ? 1e-10 : -1e-10`; S_K is never zero after the entropy fix,
+    // so the difference is never -0)
     f2 cd = p_sub(SK, Ss);
-    cd = mk2(fabsf(cd.x) < 1e-10f ? (cd.x >= 0.0f ? 1e-10f : -1e-10f) : cd.x,
-             fabsf(cd.y) < 1e-10f ? (cd.y >= 0.0f ? 1e-10f : -1e-10f) : cd.y);
+    cd = mk2(copysignf(fmaxf(fabsf(cd.x), 1e-10f), cd.x), copysignf(fmaxf(fabsf(cd.y), 1e-10f), cd.y));
     const f2 icd = p_rcp(cd);
     const f2 rs = p_max(p_mul(rkd, icd), MIN_DENSITY);
     const f2 ps = p_max(p_fma(rkd, p_sub(Ss, nK), pK), MIN_PRESSURE);
@@ -171,16 +174,18 @@ __device__ __forceinline__ void face_pair_core(bool valid0, bool near0, bool val
     const f2 F4 = p_sel(uf.x >= 0.0f, uf.y >= 0.0f, p_mul(eL, nL), p_mul(eR, nR));
     const f2 Fx = XDIR ? Fn : Ft, Fy = XDIR ? Ft : Fn;
     // wall faces: no mass/energy flux, normal momentum flux = pressure of the left/bottom cell
-    f0[0] = valid0 ? F0.x : 0.0f;
-    f0[1] = valid0 ? Fx.x : (XDIR ? a.p.x : 0.0f);
-    f0[2] = valid0 ? Fy.x : (XDIR ? 0.0f : a.p.x);
-    f0[3] = valid0 ? F3.x : 0.0f;
-    f0[4] = valid0 ? F4.x : 0.0f;
-    f1[0] = valid1 ? F0.y : 0.0f;
-    f1[1] = valid1 ? Fx.y : (XDIR ? a.p.y : 0.0f);
-    f1[2] = valid1 ? Fy.y : (XDIR ? 0.0f : a.p.y);
-    f1[3] = valid1 ? F3.y : 0.0f;
-    f1[4] = valid1 ? F4.y : 0.0f;
+    const f2 zero = splat(0.0f);
+    F[0] = p_sel(valid0, valid1, F0, zero);
+    F[1] = p_sel(valid0, valid1, Fx, XDIR ? a.p : zero);
+    F[2] = p_sel(valid0, valid1, Fy, XDIR ? zero : a.p);
+    F[3] = p_sel(valid0, valid1, F3, zero);
+    F[4] = p_sel(valid0, valid1, F4, zero);
+}
+
+// The scalar per-lane fluxes of the AUSM+ path as lane pairs.
+__device__ __forceinline__ void pair_from_lanes(const float f0[5], const float f1[5], f2 F[5]) {
+#pragma unroll
+    for (int k = 0; k < 5; k++) F[k] = mk2(f0[k], f1[k]);
 }
 
 // Limited x-slopes of a row pair from the slope ring's interleaved entries
@@ -189,52 +194,130 @@ __device__ __forceinline__ PairSl pair_sl(const float4 &A, const float4 &B) {
     return PairSl{mk2(A.x, A.y), mk2(A.z, A.w), mk2(B.x, B.y), mk2(B.z, B.w)};
 }
 
-// x-faces of rows r (lane .x -> f0) and r+1 (lane .y -> f1) between cells
-// a | b from their primitives and limited x-slopes sa, sb.
+// x-faces of rows r (lane .x) and r+1 (lane .y) between cells a | b from
+// their primitives and limited x-slopes sa, sb.
 template <int SCHEME>
 __device__ __forceinline__ void face_pair_x_sl(bool valid0, bool near0, bool valid1, bool near1, const PairPrim &a,
-                                               const PairSl &sa, const PairPrim &b, const PairSl &sb, float f0[5],
-                                               float f1[5]) {
+                                               const PairSl &sa, const PairPrim &b, const PairSl &sb, f2 F[5]) {
     if (SCHEME != 0) {  // AUSM+: per lane through the scalar path
+        float f0[5], f1[5];
         const float sa0[4] = {sa.rho.x, sa.n.x, sa.t.x, sa.p.x}, sb0[4] = {sb.rho.x, sb.n.x, sb.t.x, sb.p.x};
         const float sa1[4] = {sa.rho.y, sa.n.y, sa.t.y, sa.p.y}, sb1[4] = {sb.rho.y, sb.n.y, sb.t.y, sb.p.y};
         face_flux_sl<true, SCHEME>(valid0, near0, Prim{a.rho.x, a.u.x, a.v.x, a.p.x}, sa0,
                                    Prim{b.rho.x, b.u.x, b.v.x, b.p.x}, sb0, f0);
         face_flux_sl<true, SCHEME>(valid1, near1, Prim{a.rho.y, a.u.y, a.v.y, a.p.y}, sa1,
                                    Prim{b.rho.y, b.u.y, b.v.y, b.p.y}, sb1, f1);
+        pair_from_lanes(f0, f1, F);
         return;
     }
-    face_pair_core<true>(valid0, near0, valid1, near1, a, sa, b, sb, f0, f1);
+    face_pair_core<true>(valid0, near0, valid1, near1, a, sa, b, sb, F);
 }
 
 // The two y-faces a stage-kernel thread evaluates per step, (r-2 | r-1) in
-// lane .x -> f0 and (r-1 | r) in lane .y -> f1, from the primitives of rows
+// lane .x and (r-1 | r) in lane .y, from the primitives of rows
 // (r-2, r-1) = lo, (r-1, r) = mid and (r, r+1) = hi of one column and the
 // y-slopes of row r-2 (carried from the previous step; `sy_lo` in, the slopes
 // of row r out for the next step).
 template <int SCHEME, int LIM>
 __device__ __forceinline__ void face_pair_y(bool valid0, bool near0, bool valid1, bool near1, const PairPrim &lo,
-                                            const PairPrim &mid, const PairPrim &hi, float sy_lo[4], float f0[5],
-                                            float f1[5]) {
+                                            const PairPrim &mid, const PairPrim &hi, float sy_lo[4], f2 F[5]) {
     // slopes of rows (r-1, r): limited(row-1, row, row+1), face frame (v normal, u tangential)
     const PairSl sm{p_slope<LIM>(lo.rho, mid.rho, hi.rho), p_slope<LIM>(lo.v, mid.v, hi.v),
                     p_slope<LIM>(lo.u, mid.u, hi.u), p_slope<LIM>(lo.p, mid.p, hi.p)};
     // slopes of rows (r-2, r-1)
     const PairSl sl{mk2(sy_lo[0], sm.rho.x), mk2(sy_lo[1], sm.n.x), mk2(sy_lo[2], sm.t.x), mk2(sy_lo[3], sm.p.x)};
     if (SCHEME != 0) {  // AUSM+: per lane through the scalar path
+        float f0[5], f1[5];
         const float sa0[4] = {sl.rho.x, sl.n.x, sl.t.x, sl.p.x}, sb0[4] = {sm.rho.x, sm.n.x, sm.t.x, sm.p.x};
         const float sb1[4] = {sm.rho.y, sm.n.y, sm.t.y, sm.p.y};
         face_flux_sl<false, SCHEME>(valid0, near0, Prim{lo.rho.x, lo.u.x, lo.v.x, lo.p.x}, sa0,
                                     Prim{mid.rho.x, mid.u.x, mid.v.x, mid.p.x}, sb0, f0);
         face_flux_sl<false, SCHEME>(valid1, near1, Prim{lo.rho.y, lo.u.y, lo.v.y, lo.p.y}, sb0,
                                     Prim{mid.rho.y, mid.u.y, mid.v.y, mid.p.y}, sb1, f1);
+        pair_from_lanes(f0, f1, F);
     } else {
-        face_pair_core<false>(valid0, near0, valid1, near1, lo, sl, mid, sm, f0, f1);
+        face_pair_core<false>(valid0, near0, valid1, near1, lo, sl, mid, sm, F);
     }
     sy_lo[0] = sm.rho.y;
     sy_lo[1] = sm.n.y;
     sy_lo[2] = sm.t.y;
     sy_lo[3] = sm.p.y;
+}
+
+// Face velocities of the rho_e source for two faces (lanes): mass flux over
+// the mean of the two cells' clamped densities (src/solver.cu:1772-1794).
+__device__ __forceinline__ f2 p_face_velocity(f2 mass, f2 rho_a, f2 rho_b) {
+    const f2 mean = p_mul(splat(0.5f), p_add(p_max(rho_a, MIN_DENSITY), p_max(rho_b, MIN_DENSITY)));
+    return p_mul(mass, p_rcp(mean));
+}
+
+// Rollback of one updated cell (src/solver.cu:1812-1824): a non-finite or
+// too small density takes the old one (clamped), a non-finite momentum or
+// energy the old value, a non-finite or too small rho_e the old rho_e.  The
+// density is >= MIN_DENSITY afterwards, so the reference's second clamp to
+// MIN_DENSITY changes nothing and is left out.
+__device__ __forceinline__ void rollback_lane(float &rho, float &ru, float &rv, float &E, float &re, float U0, float U1,
+                                              float U2, float U3, float U4) {
+    if (!isfinite(rho) || rho < MIN_DENSITY) rho = fmaxf(U0, MIN_DENSITY);
+    if (!isfinite(ru)) ru = U1;
+    if (!isfinite(rv)) rv = U2;
+    if (!isfinite(E)) E = U3;
+    if (!isfinite(re) || re < MIN_PRESSURE / (GAMMA - 1.0f)) re = U4;
+}
+
+// |u| > MAX_VEL (compared in squares): velocity rescaled to MAX_VEL, momenta
+// and |u|^2 recomputed (src/solver.cu:1827-1839).
+__device__ __forceinline__ void velocity_cap_lane(float rho, float &u, float &v, float &ru, float &rv, float &q) {
+    if (q > MAX_VEL * MAX_VEL) {
+        const float scale = MAX_VEL / sqrtf(q);
+        u *= scale;
+        v *= scale;
+        ru = rho * u;
+        rv = rho * v;
+        q = u * u + v * v;
+    }
+}
+
+// updateKernel body (src/solver.cu:1736-1875) for the two cells of one
+// column in rows j (lane .x) and j+1 (lane .y), not walls: U - (dt/dx) dX -
+// (dt/dy) dY with dX = F(i+1/2) - F(i-1/2), dY = F(j+1/2) - F(j-1/2) per
+// field; the reference zeroes a flux difference across a domain edge
+// (i = 0 or nx-1 for x, j = 0 or ny-1 for y), done here by zeroing its
+// coefficient.  The rho_e source -p div(v) (interior cells) takes du =
+// u(i+1/2) - u(i-1/2) and dv = v(j+1/2) - v(j-1/2) of the face velocities
+// and p_c, the cells' primitive pressures.  Then the rollback, the velocity
+// cap and the dual-energy resync with e in [rho R T_min, rho R T_max]/(gamma-1).
+__device__ __forceinline__ void update_pair(const f2 U[5], const f2 dX[5], const f2 dY[5], f2 du, f2 dv, f2 p_c,
+                                            bool edge_x, bool edge_y0, bool edge_y1, const UpdateArgs &a,
+                                            f2 out[5]) {
+    const f2 ncx = splat(edge_x ? -0.0f : -(a.dt * a.inv_dx));
+    const f2 ncy = mk2(edge_y0 ? -0.0f : -(a.dt * a.inv_dy), edge_y1 ? -0.0f : -(a.dt * a.inv_dy));
+    f2 n[5];
+#pragma unroll
+    for (int k = 0; k < 5; k++) n[k] = p_fma(ncy, dY[k], p_fma(ncx, dX[k], U[k]));
+    const f2 div_v = p_fma(du, splat(a.inv_dx), p_mul(dv, splat(a.inv_dy)));
+    const f2 n4s = p_fma(p_mul(p_c, div_v), splat(-a.dt), n[4]);
+    n[4] = p_sel(!edge_x && !edge_y0, !edge_x && !edge_y1, n4s, n[4]);
+    rollback_lane(n[0].x, n[1].x, n[2].x, n[3].x, n[4].x, U[0].x, U[1].x, U[2].x, U[3].x, U[4].x);
+    rollback_lane(n[0].y, n[1].y, n[2].y, n[3].y, n[4].y, U[0].y, U[1].y, U[2].y, U[3].y, U[4].y);
+    const f2 rho = n[0];
+    f2 ru = n[1], rv = n[2];
+    const f2 E = n[3], re = n[4];
+    const f2 inv_rho = p_rcp(rho);
+    f2 u = p_mul(ru, inv_rho), v = p_mul(rv, inv_rho);
+    f2 q = p_fma(u, u, p_mul(v, v));
+    velocity_cap_lane(rho.x, u.x, v.x, ru.x, rv.x, q.x);
+    velocity_cap_lane(rho.y, u.y, v.y, ru.y, rv.y, q.y);
+    const f2 ke = p_mul(p_mul(splat(0.5f), rho), q);
+    const f2 e_from_E = p_sub(E, ke);
+    const f2 thr = p_mul(splat(ETA_THRESHOLD), E);  // dual-energy switch rho_e < 1e-3 E, E > 0
+    f2 e = p_sel(E.x > 0.0f && re.x < thr.x, E.y > 0.0f && re.y < thr.y, re, e_from_E);
+    e = p_min(p_max(e, p_mul(rho, splat(kEminPerRho))), p_mul(rho, splat(kEmaxPerRho)));
+    out[0] = rho;
+    out[1] = ru;
+    out[2] = rv;
+    out[3] = p_add(e, ke);
+    out[4] = e;
 }
 
 // Divergence terms of the viscous half step for one interior fluid cell

@@ -124,9 +124,10 @@ struct StageLayout {
     static constexpr size_t s_off = p_off + p_bytes;
     static constexpr size_t s_bytes = (size_t)2 * NT * 16;
     static constexpr size_t x_off = s_off + s_bytes;
-    // per face: {mass, x-mom, y-mom, energy} as a float4 plane, then {rho_e
-    // flux, face velocity} as a float2 plane, one entry per column and row
-    static constexpr size_t x_bytes = (size_t)XP * 2 * NT * (16 + 8);
+    // x-faces of a row pair, interleaved like the primitives: per column
+    // {mass_r, mass_r+1, x-mom_r, x-mom_r+1}, {y-mom, energy}, {rho_e flux,
+    // face velocity}, three float4 planes
+    static constexpr size_t x_bytes = (size_t)XP * 3 * NT * 16;
     static constexpr size_t m_off = x_off + x_bytes;
     static constexpr size_t m_bytes = (size_t)PP * 2 * NT;
     static constexpr size_t bar_off = (m_off + m_bytes + 15) & ~(size_t)15;
@@ -191,8 +192,9 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
     // normal u, tangential v): SA = {rho_r, rho_r+1, u_r, u_r+1}, SB = {v, p}
     float4 *SA = reinterpret_cast<float4 *>(smem + L::s_off);
     float4 *SB = SA + NT;
-    float4 *X4 = reinterpret_cast<float4 *>(smem + L::x_off);  // [row h][column]
-    float2 *X2 = reinterpret_cast<float2 *>(X4 + 2 * NT);       // [row h][column]
+    float4 *XA = reinterpret_cast<float4 *>(smem + L::x_off);  // [column]: mass, x-momentum
+    float4 *XB = XA + NT;                                         // y-momentum, energy
+    float4 *XC = XB + NT;                                         // rho_e flux, face velocity
     uint8_t *M = smem + L::m_off;
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bar_off);
     uint64_t *bbar = bars + KP;  // blend pair (stage 2)
@@ -290,73 +292,76 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
         // column cy, rows r-3 .. r: pairs q-2 (rows r-4, r-3), q-1 (r-2, r-1), q (r, r+1)
         const float4 A1 = PA[s1 * NT + cy], B1 = PB[s1 * NT + cy];
         const float4 A0 = PA[s0 * NT + cy], B0 = PB[s0 * NT + cy];
-        const float4 c2 = make_float4(A1.x, A1.z, B1.x, B1.z);        // row r-2 (rho, u, v, p)
-        const float4 c1 = make_float4(A1.y, A1.w, B1.y, B1.w);        // row r-1
-        const float rho0 = A0.x;                                      // density of row r
-        float fy0[5], fy1[5];
+        // y-faces (r-2 | r-1), (r-1 | r) as one lane pair; the y-slopes of row
+        // r-2 are those of row r in step q-1
+        const uint32_t my0 = M[pc1 * NT + cy], my1 = M[(pc1 + 1) * NT + cy];
+        const PairPrim lo = pair_prim(A1, B1), hi = pair_prim(A0, B0);
+        const PairPrim mid{mk2(A1.y, A0.x), mk2(A1.w, A0.z), mk2(B1.y, B0.x), mk2(B1.w, B0.z)};
+        f2 Fy[5];
+        face_pair_y<SCHEME, LIM>((my0 & MB_YV) != 0, (my0 & MB_YN) != 0, (my1 & MB_YV) != 0, (my1 & MB_YN) != 0, lo,
+                                 mid, hi, sy2, Fy);
+        // their face velocities (the face below row r-2 is carried)
+        const f2 vfy = p_face_velocity(Fy[0], lo.rho, mid.rho);
         {
-            // y-faces (r-2 | r-1) and (r-1 | r) as one lane pair; the y-slopes
-            // of row r-2 are those of row r in step q-1
-            const uint32_t my0 = M[pc1 * NT + cy], my1 = M[(pc1 + 1) * NT + cy];
-            const PairPrim lo = pair_prim(A1, B1), hi = pair_prim(A0, B0);
-            const PairPrim mid{mk2(A1.y, A0.x), mk2(A1.w, A0.z), mk2(B1.y, B0.x), mk2(B1.w, B0.z)};
-            face_pair_y<SCHEME, LIM>((my0 & MB_YV) != 0, (my0 & MB_YN) != 0, (my1 & MB_YV) != 0, (my1 & MB_YN) != 0,
-                                     lo, mid, hi, sy2, fy0, fy1);
-        }
-        // face velocities of the two y-faces (the face below row r-2 is carried)
-        const float vf0 = face_velocity(fy0[0], c2.x, c1.x), vf1 = face_velocity(fy1[0], c1.x, rho0);
+            const int u0 = r - 2;  // rows u0 (lane .x) and u0+1 (lane .y)
+            const bool st0 = col_ok && u0 >= j0 && u0 < j1, st1 = col_ok && u0 + 1 >= j0 && u0 + 1 < j1;
+            if (st0 || st1) {
+                const float *src = raw + (size_t)(ku * 2) * L::SLOT;
+                f2 Uc[5], Un[5];
 #pragma unroll
-        for (int h = 0; h < 2; h++) {
-            const int urow = r - 2 + h;
-            if (urow >= j0 && urow < j1 && col_ok) {
-                const uint32_t mb = M[(pc1 + h) * NT + cy];
-                const float *src = raw + (size_t)(ku * 2 + h) * L::SLOT;
-                const bool edge_y = (urow == 0 || urow == ny - 1);
-                float Uc[5], Un[5];
+                for (int k = 0; k < 5; k++)
+                    Uc[k] = mk2(ring_at<L::NB>(src, k, t + 4), ring_at<L::NB>(src + L::SLOT, k, t + 4));
+                // flux differences: x from the x-face ring (step q-1), y
+                // from this step's faces and the carried one below
+                const float4 LA = XA[t], RA = XA[t + 1], LB = XB[t], RB = XB[t + 1], LC = XC[t], RC = XC[t + 1];
+                const f2 dX[5] = {p_sub(mk2(RA.x, RA.y), mk2(LA.x, LA.y)), p_sub(mk2(RA.z, RA.w), mk2(LA.z, LA.w)),
+                                  p_sub(mk2(RB.x, RB.y), mk2(LB.x, LB.y)), p_sub(mk2(RB.z, RB.w), mk2(LB.z, LB.w)),
+                                  p_sub(mk2(RC.x, RC.y), mk2(LC.x, LC.y))};
+                const f2 du = p_sub(mk2(RC.z, RC.w), mk2(LC.z, LC.w));
+                f2 dY[5];
 #pragma unroll
-                for (int k = 0; k < 5; k++) Uc[k] = ring_at<L::NB>(src, k, t + 4);
-                if (mb & MB_WALL) {
+                for (int k = 0; k < 5; k++) dY[k] = mk2(Fy[k].x - fyB[k], Fy[k].y - Fy[k].x);
+                const f2 dv = mk2(vfy.x - vfB, vfy.y - vfy.x);
+                const bool ey0 = (u0 == 0 || u0 == ny - 1), ey1 = (u0 + 1 == 0 || u0 + 1 == ny - 1);
+                update_pair(Uc, dX, dY, du, dv, mk2(B1.z, B1.w), edge_x, ey0, ey1, ua, Un);
+                // wall cells keep their state
+                const bool w0 = (my0 & MB_WALL) != 0, w1 = (my1 & MB_WALL) != 0;
+                if (w0 || w1) {
 #pragma unroll
-                    for (int k = 0; k < 5; k++) Un[k] = Uc[k];
-                } else {
-                    const float4 L4 = X4[h * NT + t], R4 = X4[h * NT + t + 1];
-                    const float2 L2 = X2[h * NT + t], R2 = X2[h * NT + t + 1];
-                    const float fR[5] = {R4.x, R4.y, R4.z, R4.w, R2.x};
-                    const float fL[5] = {L4.x, L4.y, L4.z, L4.w, L2.x};
-                    float fT[5], fB[5];
-#pragma unroll
-                    for (int k = 0; k < 5; k++) {
-                        fT[k] = h ? fy1[k] : fy0[k];
-                        fB[k] = h ? fy0[k] : fyB[k];
-                    }
-                    const float4 pc = h ? c1 : c2;
-                    const float vT = h ? vf1 : vf0, vB = h ? vf0 : vfB;
-                    update_cell(Uc, fR, fL, fT, fB, R2.y, L2.y, vT, vB, pc.w, edge_x, edge_y, !edge_x && !edge_y,
-                                ua, Un);
+                    for (int k = 0; k < 5; k++) Un[k] = p_sel(w0, w1, Uc[k], Un[k]);
                 }
                 if (STAGE == 2) {
-                    const float *b = bl + (size_t)h * L::BSLOT + t;
+                    const float *b = bl + t;
 #pragma unroll
-                    for (int k = 0; k < 5; k++) Un[k] = 0.5f * b[k * W] + 0.5f * Un[k];
+                    for (int k = 0; k < 5; k++)
+                        Un[k] = p_fma(splat(0.5f), Un[k], p_mul(splat(0.5f), mk2(b[k * W], b[L::BSLOT + k * W])));
                 }
-                const uint32_t ctype = mb_type(mb);
-                // phase-1 conditions act only on non-fluid cells and the domain's edge cells
-                if (a.apply_bc && (ctype != CT_FLUID || edge_x || edge_y))
-                    bc_pointwise(Un, ctype, iu, urow, nx, ny, a.fs);
-                if (a.cfl && ctype != CT_GHOST) {
-                    float uu, vv, pp, TT;
-                    prim_from_cons(Un[0], Un[1], Un[2], Un[3], Un[4], uu, vv, pp, TT);
-                    lmax_speed = fmaxf(lmax_speed, wave_speed(uu, vv, pp, Un[0]));
-                    nbad += nonfinite5(Un);
-                }
-                float *dst = outp + (size_t)urow * g.pitch;
 #pragma unroll
-                for (int k = 0; k < 5; k++) dst[k * g.plane] = Un[k];
+                for (int h = 0; h < 2; h++) {
+                    if (!(h ? st1 : st0)) continue;
+                    const int urow = u0 + h;
+                    float Ur[5];
+#pragma unroll
+                    for (int k = 0; k < 5; k++) Ur[k] = h ? Un[k].y : Un[k].x;
+                    const uint32_t ctype = mb_type(h ? my1 : my0);
+                    // phase-1 conditions act only on non-fluid cells and the domain's edge cells
+                    if (a.apply_bc && (ctype != CT_FLUID || edge_x || (h ? ey1 : ey0)))
+                        bc_pointwise(Ur, ctype, iu, urow, nx, ny, a.fs);
+                    if (a.cfl && ctype != CT_GHOST) {
+                        float uu, vv, pp, TT;
+                        prim_from_cons(Ur[0], Ur[1], Ur[2], Ur[3], Ur[4], uu, vv, pp, TT);
+                        lmax_speed = fmaxf(lmax_speed, wave_speed(uu, vv, pp, Ur[0]));
+                        nbad += nonfinite5(Ur);
+                    }
+                    float *dst = outp + (size_t)urow * g.pitch;
+#pragma unroll
+                    for (int k = 0; k < 5; k++) dst[k * g.plane] = Ur[k];
+                }
             }
         }
 #pragma unroll
-        for (int k = 0; k < 5; k++) fyB[k] = fy1[k];
-        vfB = vf1;
+        for (int k = 0; k < 5; k++) fyB[k] = Fy[k].y;
+        vfB = vfy.y;
         // x-slopes of rows r, r+1 at staged column t+1 (columns 1 .. NT-2 are
         // the cells beside the x-faces of phase 3)
         if (t < NT - 2) {
@@ -380,18 +385,18 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
         }
         // ---- phase 3: x-faces of rows r, r+1 (read by the update in step q+1)
         {
-            float fx0[5], fx1[5];
+            f2 Fx[5];
             const float4 *A = PA + s0 * NT, *B = PB + s0 * NT;
             const uint32_t mb0 = M[pc0 * NT + tx + 1], mb1 = M[(pc0 + 1) * NT + tx + 1];
-            face_pair_x_sl<SCHEME>((mb0 & MB_XV) != 0, (mb0 & MB_XN) != 0, (mb1 & MB_XV) != 0, (mb1 & MB_XN) != 0,
-                                   pair_prim(A[tx + 1], B[tx + 1]), pair_sl(SA[tx + 1], SB[tx + 1]),
-                                   pair_prim(A[tx + 2], B[tx + 2]), pair_sl(SA[tx + 2], SB[tx + 2]), fx0, fx1);
+            const PairPrim ca = pair_prim(A[tx + 1], B[tx + 1]), cb = pair_prim(A[tx + 2], B[tx + 2]);
+            face_pair_x_sl<SCHEME>((mb0 & MB_XV) != 0, (mb0 & MB_XN) != 0, (mb1 & MB_XV) != 0, (mb1 & MB_XN) != 0, ca,
+                                   pair_sl(SA[tx + 1], SB[tx + 1]), cb, pair_sl(SA[tx + 2], SB[tx + 2]), Fx);
             if (t <= W) {
-                X4[t] = make_float4(fx0[0], fx0[1], fx0[2], fx0[3]);
-                X4[NT + t] = make_float4(fx1[0], fx1[1], fx1[2], fx1[3]);
+                XA[t] = make_float4(Fx[0].x, Fx[0].y, Fx[1].x, Fx[1].y);
+                XB[t] = make_float4(Fx[2].x, Fx[2].y, Fx[3].x, Fx[3].y);
                 // with the face velocities for the rho_e source of both adjacent cells
-                X2[t] = make_float2(fx0[4], face_velocity(fx0[0], A[tx + 1].x, A[tx + 2].x));
-                X2[NT + t] = make_float2(fx1[4], face_velocity(fx1[0], A[tx + 1].y, A[tx + 2].y));
+                const f2 vel = p_face_velocity(Fx[0], ca.rho, cb.rho);
+                XC[t] = make_float4(Fx[4].x, Fx[4].y, vel.x, vel.y);
             }
         }
         pc1 = pc0;

@@ -9,8 +9,15 @@
 * Hypersonic blunted cone (Mach 8, Re 1e5, isothermal wall) on a reduced
   512x256 grid: bow-shock standoff, integrated wall heat flux and drag within
   0.5 % of the FP64 oracle after 2000 steps.
-Both solves use the recompute-dt policy (each step's dt from the CFL of its
-start state) and start from the same geometry and state."""
+* The same blunted cone inviscid (Euler, slip wall) run to a steady bow shock
+  on 1024x512, 2048x1024 and 4096x2048 grids: the standoff on the axis
+  converges with the grid toward Billig's correlation for cylinder-nosed
+  bodies (F. S. Billig, J. Spacecraft Rockets 4(6):822-823, 1967: standoff /
+  nose radius = 0.386 exp(4.67 / M^2), 0.4152 at Mach 8), a published
+  reference for the hypersonic path, which has no reference counterpart.
+The oracle comparisons use the recompute-dt policy (each step's dt from the
+CFL of its start state) and start from the same geometry and state."""
+import math
 import os
 
 import numpy as np
@@ -109,3 +116,33 @@ def test_cone_standoff_heat_and_drag_match_fp64_oracle():
     assert abs(dg.cd - do.cd) <= 5e-3 * abs(do.cd), (dg.cd, do.cd)
     # FP32 state, FP64 totals: mass drifts from the FP64 solve by < 1e-3 over 2000 steps
     assert abs(dg.mass - do.mass) <= 1e-3 * do.mass
+
+
+def _steady_inviscid_standoff(nx, ny, flow_radii=40.0):
+    """Standoff / nose radius of the inviscid Mach-8 cone after `flow_radii`
+    nose radii of freestream travel (steady from ~30 on)."""
+    p, e = abi.workload("ns_hypersonic_cone", nx, ny)
+    p.enable_viscosity = False
+    e.dt_policy = abi.DT_RECOMPUTE
+    with fvm_b200.Solver(p, e) as s:
+        rn = p.obstacle_r
+        chunk = 1000 * nx // 1024
+        while s.params.t_current * p.u_inf / rn < flow_radii:
+            s.step(chunk)
+        assert np.isfinite(s.fields()).all()
+        return s.shock_standoff() / rn
+
+
+def test_inviscid_cone_standoff_converges_to_billig_correlation():
+    billig = 0.386 * math.exp(4.67 / 8.0 ** 2)
+    d = [_steady_inviscid_standoff(nx, nx // 2) for nx in (1024, 2048, 4096)]
+    err = [x / billig - 1.0 for x in d]
+    # the error falls with every refinement (the captured shock is a few
+    # cells wide, which moves the pressure midpoint upstream on coarse grids)
+    assert abs(err[2]) < abs(err[1]) < abs(err[0]), d
+    assert abs(err[2]) < 0.08, d
+    # Richardson extrapolation with the observed order of the three grids
+    r = (d[1] - d[2]) / (d[0] - d[1])
+    assert 0.0 < r < 1.0, d
+    d_inf = d[2] - (d[1] - d[2]) * r / (1.0 - r)
+    assert abs(d_inf / billig - 1.0) < 0.05, (d, d_inf, billig)

@@ -143,7 +143,11 @@ int fvm_set_ext(fvm_handle *h, const fvm_ext *ext);
  * work is queued; a device error of those steps is reported by the next
  * fvm_synchronize (or the next call that reads device scalars). */
 int fvm_step(fvm_handle *h, fvm_sim_params *p);
-/* n steps back to back (graph-captured after the first call for a given shape). */
+/* n steps back to back.  On a non-default stream the steps replay captured
+ * CUDA graphs (two steps per graph, one-step graphs for an odd remainder and
+ * for fvm_step); the first call that needs a graph kind captures it for both
+ * ping-pong buffer parities, and a change of launch shape, dt policy, CFL
+ * numbers, viscosity switches or stream captures them again. */
 int fvm_steps(fvm_handle *h, fvm_sim_params *p, int n);
 /* CFDSolver::computeStableTimeStep (src/solver.cu:3273-3278). */
 int fvm_compute_dt(fvm_handle *h, const fvm_sim_params *p, float *dt_out);

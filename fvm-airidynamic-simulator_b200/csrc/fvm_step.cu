@@ -213,25 +213,24 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
     __syncthreads();
     const int base = rp.base;  // row pairs this CTA staged before this tile
     const int bbase = rp.bbase;
-    int islot = base % KP;
+    // stage input row pair q of this tile into its slot (base + q) % KP
     auto issue = [&](int q) {
-        mbar_arrive_expect_tx(&bars[islot], L::tx_bytes);
+        const int slot = (base + q) % KP;
+        mbar_arrive_expect_tx(&bars[slot], L::tx_bytes);
 #pragma unroll
         for (int h = 0; h < 2; h++) {
             const int row = clampi(rs + 2 * q + h, 0, ny - 1);
-            float *dst = raw + (size_t)(islot * 2 + h) * L::SLOT;
+            float *dst = raw + (size_t)(slot * 2 + h) * L::SLOT;
 #pragma unroll
             for (int b = 0; b < L::NB; b++)
-                tma_load_3d(dst + b * kBoxStride, tm_in, &bars[islot], i0 - 4 + b * kBox, row, 0);
+                tma_load_3d(dst + b * kBoxStride, tm_in, &bars[slot], i0 - 4 + b * kBox, row, 0);
         }
-        islot = ring_next<KP>(islot);
     };
     // blend partner rows of pair p (updated in step p+1; pair 0 and the last
     // pair are never updated)
     const int nblend = STAGE == 2 ? max(0, npairs - 2) : 0;
-    int bissued = 0;  // blend pairs staged in this tile (thread 0's count)
+    int bissued = 0;  // blend pairs staged in this tile (the same count in every thread)
     auto issue_blend = [&](int p) {
-        ++bissued;
         mbar_arrive_expect_tx(bbar, L::btx_bytes);
 #pragma unroll
         for (int h = 0; h < 2; h++)
@@ -375,13 +374,19 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
         fence_proxy_async_smem();
         __syncthreads();
         // the input slot of pair q-1 is free now: stage pair q-1+KP into it;
-        // the blend slot too: stage the blend rows of pair q
-        if (t == 0) {
+        // the blend slot too: stage the blend rows of pair q.  Lane 0 of warp
+        // q mod (NT/32) issues, so no warp carries the issue work every step
+        // (the barriers wait for the slowest warp)
+        {
+            const int who = (q % (NT / 32)) * 32;
             if (issued < npairs && issued <= q + KP - 1) {
-                issue(issued);
+                if (t == who) issue(issued);
                 ++issued;
             }
-            if (STAGE == 2 && q >= 1 && q <= nblend) issue_blend(q);
+            if (STAGE == 2 && q >= 1 && q <= nblend) {
+                if (t == who) issue_blend(q);
+                ++bissued;
+            }
         }
         // ---- phase 3: x-faces of rows r, r+1 (read by the update in step q+1)
         {
@@ -608,6 +613,8 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
             break;
         }
         // the input slot of pair q is free now: stage pair q+KP into it
+        // (thread 0 issues; rotating the issuing warp as the stage kernels do
+        // gave this pass nothing)
         if (t == 0 && issued < npairs && issued <= q + KP) {
             issue(issued);
             ++issued;

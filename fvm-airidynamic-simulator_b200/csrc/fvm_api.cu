@@ -403,11 +403,13 @@ extern "C" int fvm_create(fvm_handle **out) {
     fvm_ext_default(&h->ext);
     if (cudaMalloc(&h->sc, sizeof(DevScalars)) != cudaSuccess || cudaMalloc(&h->d_count, sizeof(int)) != cudaSuccess ||
         cudaMalloc(&h->d_tmp, 16) != cudaSuccess || cudaMalloc(&h->d_counter, sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&h->d_disp, sizeof(DisplayDesc)) != cudaSuccess ||
         cudaMallocHost(&h->h_sc, sizeof(DevScalars)) != cudaSuccess) {
         delete h;
         return set_err(FVM_ERR_ALLOC, "fvm_create: allocation failed");
     }
     cudaMemsetAsync(h->sc, 0, sizeof(DevScalars), h->stream);
+    cudaMemsetAsync(h->d_disp, 0, sizeof(DisplayDesc), h->stream);
     cudaStreamSynchronize(h->stream);
     *out = h;
     return FVM_OK;
@@ -423,6 +425,7 @@ extern "C" int fvm_destroy(fvm_handle *h) {
     if (h->d_count) cudaFree(h->d_count);
     if (h->d_tmp) cudaFree(h->d_tmp);
     if (h->d_counter) cudaFree(h->d_counter);
+    if (h->d_disp) cudaFree(h->d_disp);
     if (h->h_sc) cudaFreeHost(h->h_sc);
     if (h->own) cudaStreamDestroy(h->own);
     delete h;
@@ -458,6 +461,7 @@ extern "C" int fvm_reset(fvm_handle *h, const fvm_sim_params *p) {
     if (p->nx != h->g.nx || p->ny != h->g.ny)
         return set_err(FVM_ERR_INVALID, "fvm_reset: grid %dx%d differs from the allocated %dx%d (use fvm_initialize)",
                        p->nx, p->ny, h->g.nx, h->g.ny);
+    h->disp_fresh = false;
     h->prm = *p;
     h->g.dx = p->dx;
     h->g.dy = p->dy;
@@ -476,6 +480,11 @@ extern "C" int fvm_reset(fvm_handle *h, const fvm_sim_params *p) {
 extern "C" int fvm_initialize(fvm_handle *h, const fvm_sim_params *p, const fvm_ext *ext) {
     CHECK_HANDLE(h);
     if (int r = validate(p, ext)) return r;
+    if (h->disp) {  // a registered display field is sized for the old grid
+        CK(launch_set_display(h->d_disp, nullptr, 0, h->stream));
+        h->disp = nullptr;
+    }
+    h->disp_fresh = false;
     h->prm = *p;
     if (ext) h->ext = *ext;
     if (int r = alloc_buffers(h, p->nx, p->ny)) return r;
@@ -487,6 +496,11 @@ extern "C" int fvm_resize(fvm_handle *h, int nx, int ny) {
     CHECK_HANDLE(h);
     if (nx <= 0 || ny <= 0) return set_err(FVM_ERR_INVALID, "fvm_resize: nx, ny must be positive");
     if (h->Un && nx == h->g.nx && ny == h->g.ny) return FVM_OK;
+    if (h->disp) {  // a registered display field is sized for the old grid
+        CK(launch_set_display(h->d_disp, nullptr, 0, h->stream));
+        h->disp = nullptr;
+    }
+    h->disp_fresh = false;
     h->prm.nx = nx;
     h->prm.ny = ny;
     if (int r = alloc_buffers(h, nx, ny)) return r;
@@ -506,6 +520,7 @@ extern "C" int fvm_set_ext(fvm_handle *h, const fvm_ext *ext) {
 extern "C" int fvm_update_obstacle(fvm_handle *h, const fvm_sim_params *p) {
     CHECK_INIT(h);
     if (int r = validate(p, nullptr)) return r;
+    h->disp_fresh = false;
     h->prm = *p;
     if (int r = build_geometry(h, true)) return r;
     if (int r = apply_bc_full(h)) return r;
@@ -567,8 +582,10 @@ static int enqueue_step(fvm_handle *h) {
         GhostArgs g1 = ghost_args(h, Us, Un, nullptr, 0, 0);
         CK(timed(h, 4, [&] { return launch_ghost(g1, st); }));
         StepArgs a2 = step_args(h, Ux, 1, 1, 1.0f);
+        a2.disp = h->disp ? h->d_disp : nullptr;
         CK(timed(h, 1, [&] { return launch_stage(2, sch, lim, tn, inS, ctrN, a2, st); }));
         GhostArgs g2 = ghost_args(h, Ux, Un, Us, 1, 1);
+        g2.disp = h->disp ? h->d_disp : nullptr;
         CK(timed(h, 5, [&] { return launch_ghost(g2, st); }));
     } else {
         StepArgs v1 = step_args(h, Ud, 0, 0, 0.5f);
@@ -581,8 +598,10 @@ static int enqueue_step(fvm_handle *h) {
         StepArgs a2 = step_args(h, Ud, 0, 0, 1.0f);
         CK(timed(h, 1, [&] { return launch_stage(2, sch, lim, tn, inS, ctrD, a2, st); }));
         StepArgs v2 = step_args(h, Ux, 1, 2, 0.5f);
+        v2.disp = h->disp ? h->d_disp : nullptr;
         CK(timed(h, 3, [&] { return launch_viscous(tn, inD, v2, st); }));
         GhostArgs g2 = ghost_args(h, Ux, Ud, nullptr, 2, 1);
+        g2.disp = h->disp ? h->d_disp : nullptr;
         CK(timed(h, 5, [&] { return launch_ghost(g2, st); }));
     }
     return FVM_OK;
@@ -628,6 +647,7 @@ static unsigned long long graph_key(fvm_handle *h) {
     k = k * 1000003ULL + (unsigned long long)h->n_ghost;
     k = k * 7 + h->ext.dt_policy;
     k = k * 1000003ULL + (unsigned long long)(uintptr_t)h->stream;
+    k = k * 3 + (h->disp != nullptr ? 1 : 0);  // display-field variants of the last passes
     uint32_t c1, c2;
     memcpy(&c1, &h->prm.cfl, 4);
     memcpy(&c2, &h->prm.cfl_visc, 4);
@@ -722,6 +742,7 @@ extern "C" int fvm_steps(fvm_handle *h, fvm_sim_params *p, int n) {
     if (!p) return set_err(FVM_ERR_INVALID, "null params");
     if (n < 0) return set_err(FVM_ERR_INVALID, "negative step count");
     if (n == 0) return FVM_OK;
+    h->disp_fresh = false;  // until every step is queued
     // per-step knobs the reference reads from params on every call
     h->prm.cfl = p->cfl;
     h->prm.cfl_visc = p->cfl_visc;
@@ -759,7 +780,9 @@ extern "C" int fvm_steps(fvm_handle *h, fvm_sim_params *p, int n) {
         if (int r = enqueue_step(h)) return r;
         swap_state(h);
     }
-    return finish_steps(h, p, n);
+    const int rf = finish_steps(h, p, n);
+    h->disp_fresh = rf == FVM_OK && h->disp != nullptr;
+    return rf;
 }
 
 extern "C" int fvm_synchronize(fvm_handle *h) {
@@ -893,6 +916,7 @@ extern "C" int fvm_read_region_geometry(fvm_handle *h, int i0, int j0, int w, in
 extern "C" int fvm_write_fields(fvm_handle *h, const float *rho, const float *rho_u, const float *rho_v,
                                 const float *E, const float *rho_e) {
     CHECK_INIT(h);
+    h->disp_fresh = false;
     const float *src[5] = {rho, rho_u, rho_v, E, rho_e};
     for (int k = 0; k < 5; k++) {
         if (!src[k]) continue;
@@ -924,8 +948,25 @@ extern "C" int fvm_field_to_device(fvm_handle *h, int kind, float *dev_dst) {
     CHECK_INIT(h);
     if (!dev_dst) return set_err(FVM_ERR_INVALID, "null destination");
     if (kind < 0 || kind > 4) return set_err(FVM_ERR_INVALID, "unknown field kind %d", kind);
+    const bool into_display = h->disp && dev_dst == h->disp;
+    // the registered display field, already written by the last step
+    if (into_display && kind == h->disp_kind && h->disp_fresh) return FVM_OK;
     CK(launch_derived(kind, h->g, h->Un, dev_dst, h->stream));
     h->launches++;
+    if (into_display) h->disp_fresh = kind == h->disp_kind;
+    return FVM_OK;
+}
+
+extern "C" int fvm_set_display_field(fvm_handle *h, int kind, float *dev_dst) {
+    CHECK_INIT(h);
+    if (dev_dst && (kind < 0 || kind > 4)) return set_err(FVM_ERR_INVALID, "unknown field kind %d", kind);
+    if (dev_dst == h->disp && (!dev_dst || kind == h->disp_kind)) return FVM_OK;
+    // the descriptor is updated in stream order, before the next step reads it
+    CK(launch_set_display(h->d_disp, dev_dst, dev_dst ? kind : 0, h->stream));
+    h->launches++;
+    h->disp = dev_dst;
+    h->disp_kind = dev_dst ? kind : 0;
+    h->disp_fresh = false;
     return FVM_OK;
 }
 
@@ -1118,6 +1159,7 @@ extern "C" int fvm_autotune(fvm_handle *h, const fvm_sim_params *p, int steps, f
     h->timing = timing;
     h->cfl_valid = false;
     h->dt_ready = false;
+    h->disp_fresh = false;  // the tuning steps wrote it; the state is restored
     if (rc != FVM_OK) return rc;
     if (r2 != FVM_OK) return r2;
     g_tune_cache[TuneKey{h->g.nx, h->g.ny, h->prm.enable_viscosity ? 1 : 0, h->ext.flux_scheme, h->ext.limiter}] =

@@ -19,33 +19,6 @@ __global__ void k_primitives(GridDesc g, const float *U, float *u, float *v, flo
     if (T) T[d] = TT;
 }
 
-// compute{Temperature,Pressure,VelocityMag,Mach}DirectKernel and the density
-// copy (src/solver.cu:3527-3671): the derived value of one cell.
-__device__ __forceinline__ float derived_value(int kind, float rho, float rho_u, float rho_v, float rho_e) {
-    switch (kind) {
-    case 0: {
-        float e = rho_e / (rho + 1e-10f);
-        return (GAMMA - 1.0f) * e / R_GAS;
-    }
-    case 1: return (GAMMA - 1.0f) * rho_e;
-    case 2: return rho;
-    case 3: {
-        float rv = rho + 1e-10f;
-        float u = rho_u / rv, v = rho_v / rv;
-        return sqrtf(u * u + v * v);
-    }
-    default: {
-        float rv = rho + 1e-10f;
-        float u = rho_u / rv, v = rho_v / rv;
-        float speed = sqrtf(u * u + v * v);
-        float e = rho_e / rv;
-        float T = (GAMMA - 1.0f) * e / R_GAS;
-        float cs = sqrtf(GAMMA * R_GAS * T);
-        return speed / (cs + 1e-10f);
-    }
-    }
-}
-
 // Derived field into a dense nx*ny destination.
 __global__ void k_derived(int kind, GridDesc g, const float *U, float *dst) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;

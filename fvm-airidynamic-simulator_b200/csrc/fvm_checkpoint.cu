@@ -171,6 +171,7 @@ extern "C" int fvm_load_checkpoint(fvm_handle *h, const char *path, fvm_sim_para
     h->dt_ready = (hd.flags & kFlagDtReady) != 0;
     h->fixed_dt = hd.next_dt;
     h->cfl_valid = (hd.flags & kFlagCflValid) != 0;
+    h->disp_fresh = false;
     if (p_out) *p_out = hd.params;
     return FVM_OK;
 }

@@ -53,6 +53,14 @@ struct fvm_handle {
     // graph replay of one step (single-step calls and odd remainders), per parity
     cudaGraphExec_t graph1[2] = {nullptr, nullptr};
     unsigned long long graph1_key[2] = {0, 0};
+    // registered display field (fvm_set_display_field): the last passes of
+    // every step write it (destination and kind in the device descriptor
+    // d_disp, mirrored in disp / disp_kind); fresh while the state is the one
+    // a step (or a derived-field pass into it) left
+    DisplayDesc *d_disp = nullptr;
+    float *disp = nullptr;
+    int disp_kind = 0;
+    bool disp_fresh = false;
     float fixed_dt = 0.0f;       // fixed policy: the dt sc->dt holds when dt_ready
     float *parity_base = nullptr;  // buffer holding U^n at parity 0
     // measurement

@@ -50,6 +50,45 @@ struct DevScalars {
     double diag[16];  // FP64 diagnostic accumulators
 };
 
+// compute{Temperature,Pressure,VelocityMag,Mach}DirectKernel and the density
+// copy (src/solver.cu:3527-3671): the derived value of one cell (kind =
+// FVM_FIELD_*).  Used by the derived-field pass and, for a registered display
+// field, by the last passes of a step.
+__device__ __forceinline__ float derived_value(int kind, float rho, float rho_u, float rho_v, float rho_e) {
+    switch (kind) {
+    case 0: {
+        float e = rho_e / (rho + 1e-10f);
+        return (GAMMA - 1.0f) * e / R_GAS;
+    }
+    case 1: return (GAMMA - 1.0f) * rho_e;
+    case 2: return rho;
+    case 3: {
+        float rv = rho + 1e-10f;
+        float u = rho_u / rv, v = rho_v / rv;
+        return sqrtf(u * u + v * v);
+    }
+    default: {
+        float rv = rho + 1e-10f;
+        float u = rho_u / rv, v = rho_v / rv;
+        float speed = sqrtf(u * u + v * v);
+        float e = rho_e / rv;
+        float T = (GAMMA - 1.0f) * e / R_GAS;
+        float cs = sqrtf(GAMMA * R_GAS * T);
+        return speed / (cs + 1e-10f);
+    }
+    }
+}
+
+// A registered display field of one solve: the destination of the derived
+// field the last passes of every step write (null: none), read by the
+// kernels at run time so that captured step graphs stay valid when the
+// application registers another buffer.
+struct DisplayDesc {
+    float *ptr;
+    int kind;
+    int pad;
+};
+
 // Step-kernel arguments common to all stage kernels.
 struct StepArgs {
     GridDesc g;
@@ -64,6 +103,7 @@ struct StepArgs {
     int apply_bc;          // phase-1 boundary conditions on the output
     int cfl;               // 0: none, 1: wave speed, 2: wave speed + kinematic viscosity
     float dt_scale;        // stage dt = sc->dt * dt_scale (0.5 for the viscous half steps)
+    const DisplayDesc *disp;  // last pass of a step: display field of the output (dense nx*ny), or null
 };
 
 struct GhostArgs {
@@ -82,6 +122,7 @@ struct GhostArgs {
     float cfl_num, cfl_visc, min_dx;
     int viscous;
     int flip_parity;       // batched solves: toggle sc->parity in the finalize
+    const DisplayDesc *disp;  // display field of the ghost cells written (dense nx*ny), or null
 };
 
 // ---------------------------------------------------------- batched solves

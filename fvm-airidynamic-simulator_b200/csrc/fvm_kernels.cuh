@@ -42,6 +42,7 @@ cudaError_t launch_viscous_batch(const StageTune &tn, const BatchInst *insts, co
 cudaError_t launch_ghost_batch(const BatchInst *insts, const GhostChunk *chunks, int nchunks, int mode,
                                cudaStream_t st);
 // Ghost-cell pass over the ghost table.
+cudaError_t launch_set_display(DisplayDesc *d, float *ptr, int kind, cudaStream_t st);
 cudaError_t launch_ghost(const GhostArgs &a, cudaStream_t st);
 // Bounded wait on an mbarrier nothing arrives on (expires after limit_cycles).
 cudaError_t launch_wait_probe(DevScalars *sc, long long limit_cycles, cudaStream_t st);

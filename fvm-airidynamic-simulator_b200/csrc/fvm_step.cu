@@ -175,7 +175,7 @@ struct RingPos {
 // barrier of step q (the update of pair q-1 has read the slot by then); the
 // update of pair q in step q+1 waits for them with the input.  Returns
 // false when a bounded wait expired (error recorded; caller must stop).
-template <int NT, int K, int STAGE, int SCHEME, int LIM>
+template <int NT, int K, int STAGE, int SCHEME, int LIM, bool DISP = false>
 __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUtensorMap *tm_blend, const StepArgs &a,
                                            int i0, int j0, unsigned char *smem, RingPos &rp, float &lmax_speed,
                                            unsigned &nbad) {
@@ -355,6 +355,13 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
                     float *dst = outp + (size_t)urow * g.pitch;
 #pragma unroll
                     for (int k = 0; k < 5; k++) dst[k * g.plane] = Ur[k];
+                    // a registered display field of the step's result (the descriptor
+                    // is read here, not held in registers across the loop)
+                    if (DISP && STAGE == 2) {
+                        float *const dptr = a.disp->ptr;
+                        if (dptr)
+                            dptr[(size_t)urow * nx + iu] = derived_value(a.disp->kind, Ur[0], Ur[1], Ur[2], Ur[4]);
+                    }
                 }
             }
         }
@@ -430,7 +437,7 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
 // Occupancy target: 6 CTAs of 128 threads per SM (80 registers, no spills;
 // ~30 KB of shared memory per CTA for stage 1, ~35 KB for stage 2 with its
 // blend pair).
-template <int NT, int K, int STAGE, int SCHEME, int LIM>
+template <int NT, int K, int STAGE, int SCHEME, int LIM, bool DISP>
 __global__ void __launch_bounds__(NT, 768 / NT)
     k_stage(const __grid_constant__ CUtensorMap tm_in, const __grid_constant__ CUtensorMap tm_blend,
             const StepArgs a) {
@@ -449,8 +456,8 @@ __global__ void __launch_bounds__(NT, 768 / NT)
     RingPos rp{0, 0};
     float lmax = 0.0f;
     unsigned nbad = 0;
-    if (!stage_tile<NT, K, STAGE, SCHEME, LIM>(&tm_in, &tm_blend, a, blockIdx.x * L::W, blockIdx.y * a.rows_per_cta,
-                                               smem, rp, lmax, nbad))
+    if (!stage_tile<NT, K, STAGE, SCHEME, LIM, DISP>(&tm_in, &tm_blend, a, blockIdx.x * L::W,
+                                                     blockIdx.y * a.rows_per_cta, smem, rp, lmax, nbad))
         return;
     if (a.cfl) block_publish<NT>(lmax, 0.0f, nbad, a.sc);
 }
@@ -502,7 +509,7 @@ struct ViscLayout {
 //            phase 1 meanwhile)
 // Both rows of a phase are evaluated in straight-line code (validity applied
 // by selects and predicated stores), so their dependency chains interleave.
-template <int NT, int K>
+template <int NT, int K, bool DISP = false>
 __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const StepArgs &a, int i0, int j0,
                                              unsigned char *smem, RingPos &rp, float &lmax_speed, float &lmax_nu,
                                              unsigned &nbad) {
@@ -725,6 +732,13 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
                     float *dst = a.out + (size_t)(r - 2 + h) * g.pitch + ic;
 #pragma unroll
                     for (int k = 0; k < 5; k++) dst[k * g.plane] = U[h][k];
+                    // a registered display field of the step's result (post pass)
+                    if (DISP) {
+                        float *const dptr = a.disp->ptr;
+                        if (dptr)
+                            dptr[(size_t)(r - 2 + h) * nx + ic] =
+                                derived_value(a.disp->kind, U[h][0], U[h][1], U[h][2], U[h][4]);
+                    }
                 }
             }
         }
@@ -760,7 +774,7 @@ __device__ __forceinline__ bool viscous_tile(const CUtensorMap *tm_in, const Ste
 // memory each): the column's own primitives and stress operands live in
 // registers across steps, which at 80 registers (6 CTAs) spilled and ran
 // 15-20 % slower.
-template <int NT, int K>
+template <int NT, int K, bool DISP>
 __global__ void __launch_bounds__(NT, 640 / NT) k_viscous(const __grid_constant__ CUtensorMap tm_in, const StepArgs a) {
     using L = ViscLayout<NT, K>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -775,7 +789,7 @@ __global__ void __launch_bounds__(NT, 640 / NT) k_viscous(const __grid_constant_
     RingPos rp{0, 0};
     float ls = 0.0f, ln = 0.0f;
     unsigned nbad = 0;
-    if (!viscous_tile<NT, K>(&tm_in, a, blockIdx.x * L::W, blockIdx.y * a.rows_per_cta, smem, rp, ls, ln, nbad))
+    if (!viscous_tile<NT, K, DISP>(&tm_in, a, blockIdx.x * L::W, blockIdx.y * a.rows_per_cta, smem, rp, ls, ln, nbad))
         return;
     if (a.cfl) block_publish<NT>(ls, ln, nbad, a.sc);
 }
@@ -808,6 +822,7 @@ __device__ __forceinline__ StepArgs batch_args(const BatchInst &I, int out_role,
     a.apply_bc = apply_bc;
     a.cfl = cfl;
     a.dt_scale = dts;
+    a.disp = nullptr;
     return a;
 }
 
@@ -964,6 +979,10 @@ __device__ __forceinline__ void ghost_chunk(const GhostArgs &a, int first, int c
     }
 #pragma unroll
     for (int f = 0; f < 5; f++) a.A[f * plane + pidx] = out[f];
+    if (a.disp) {
+        float *const dptr = a.disp->ptr;
+        if (dptr) dptr[(size_t)gi.j * a.g.nx + gi.i] = derived_value(a.disp->kind, out[0], out[1], out[2], out[4]);
+    }
     if (a.cfl) {
         float uu, vv, pp, TT;
         prim_from_cons(out[0], out[1], out[2], out[3], out[4], uu, vv, pp, TT);
@@ -1101,14 +1120,22 @@ int stage_box_blend(const StageTune &tn) { return tn.nt - 4; }
 template <int NT, int K, int STAGE, int SCHEME, int LIM>
 static cudaError_t stage_attr_t() {
     using L = StageLayout<NT, K, STAGE>;
-    return cudaFuncSetAttribute(k_stage<NT, K, STAGE, SCHEME, LIM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)L::total);
+    cudaError_t e = cudaFuncSetAttribute(k_stage<NT, K, STAGE, SCHEME, LIM, false>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::total);
+    if (STAGE == 2 && e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_stage<NT, K, STAGE, SCHEME, LIM, STAGE == 2>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::total);
+    return e;
 }
 
 template <int NT, int K>
 static cudaError_t visc_attr_t() {
-    return cudaFuncSetAttribute(k_viscous<NT, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)ViscLayout<NT, K>::total);
+    cudaError_t e = cudaFuncSetAttribute(k_viscous<NT, K, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)ViscLayout<NT, K>::total);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_viscous<NT, K, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)ViscLayout<NT, K>::total);
+    return e;
 }
 
 template <int NT, int K, int STAGE, int SCHEME, int LIM>
@@ -1148,7 +1175,9 @@ template <int NT, int K, int STAGE, int SCHEME, int LIM>
 static cudaError_t launch_stage_t(const StageTune &tn, const CUtensorMap &tm_in, const CUtensorMap &tm_blend,
                                   const StepArgs &a, cudaStream_t st) {
     using L = StageLayout<NT, K, STAGE>;
-    auto kern = k_stage<NT, K, STAGE, SCHEME, LIM>;
+    // the display-field variant only for a stage 2 that writes one
+    auto kern = (STAGE == 2 && a.disp) ? k_stage<NT, K, STAGE, SCHEME, LIM, STAGE == 2>
+                                       : k_stage<NT, K, STAGE, SCHEME, LIM, false>;
     dim3 grid((a.g.nx + L::W - 1) / L::W, (a.g.ny + a.rows_per_cta - 1) / a.rows_per_cta);
     kern<<<grid, NT, L::total, st>>>(tm_in, tm_blend, a);
     return cudaGetLastError();
@@ -1177,7 +1206,7 @@ cudaError_t launch_stage(int stage, int scheme, int limiter, const StageTune &tn
 template <int NT, int K>
 static cudaError_t launch_viscous_t(const CUtensorMap &tm_in, const StepArgs &a, cudaStream_t st) {
     using L = ViscLayout<NT, K>;
-    auto kern = k_viscous<NT, K>;
+    auto kern = a.disp ? k_viscous<NT, K, true> : k_viscous<NT, K, false>;
     dim3 grid((a.g.nx + L::W - 1) / L::W, (a.g.ny + a.rows_per_cta - 1) / a.rows_per_cta);
     kern<<<grid, NT, L::total, st>>>(tm_in, a);
     return cudaGetLastError();
@@ -1276,6 +1305,16 @@ __global__ void k_wait_probe(DevScalars *sc, long long limit) {
 
 cudaError_t launch_wait_probe(DevScalars *sc, long long limit_cycles, cudaStream_t st) {
     k_wait_probe<<<1, 32, 0, st>>>(sc, limit_cycles);
+    return cudaGetLastError();
+}
+
+__global__ void k_set_display(DisplayDesc *d, float *ptr, int kind) {
+    d->ptr = ptr;
+    d->kind = kind;
+}
+
+cudaError_t launch_set_display(DisplayDesc *d, float *ptr, int kind, cudaStream_t st) {
+    k_set_display<<<1, 1, 0, st>>>(d, ptr, kind);
     return cudaGetLastError();
 }
 

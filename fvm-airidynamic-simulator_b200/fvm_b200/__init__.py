@@ -26,7 +26,8 @@ EXPORTS = [
     "fvm_update_obstacle", "fvm_set_ext", "fvm_step", "fvm_steps", "fvm_compute_dt", "fvm_queue_dt",
     "fvm_read_dt", "fvm_synchronize", "fvm_get_cell_types", "fvm_get_sdf", "fvm_read_fields",
     "fvm_read_region", "fvm_read_region_geometry",
-    "fvm_write_fields", "fvm_read_primitives", "fvm_field_to_device", "fvm_cell_types_to_device",
+    "fvm_write_fields", "fvm_read_primitives", "fvm_field_to_device", "fvm_set_display_field",
+    "fvm_cell_types_to_device",
     "fvm_vector_arrows", "fvm_max_temperature", "fvm_max_mach", "fvm_memory_usage", "fvm_gpu_mem_info",
     "fvm_diagnostics", "fvm_shock_standoff", "fvm_set_kernel_timing", "fvm_kernel_times",
     "fvm_launch_count", "fvm_batch_create", "fvm_batch_destroy", "fvm_batch_set_stream", "fvm_batch_add",
@@ -93,6 +94,7 @@ def load_library(path=None):
     lib.fvm_write_fields.argtypes = [vp] + [vp] * 5
     lib.fvm_read_primitives.argtypes = [vp] + [vp] * 4
     lib.fvm_field_to_device.argtypes = [vp, i, vp]
+    lib.fvm_set_display_field.argtypes = [vp, i, vp]
     lib.fvm_colormap_to_device.argtypes = [vp, i, i, f, f, vp, i]
     lib.fvm_colormap_table.argtypes = [i, vp]
     lib.fvm_save_checkpoint.argtypes = [vp, Pp, C.c_char_p]
@@ -270,6 +272,11 @@ class Solver:
 
     def field_to_device(self, kind, dev_ptr):
         _check(self.lib.fvm_field_to_device(self.h, int(kind), C.c_void_p(dev_ptr)))
+
+    def set_display_field(self, kind, dev_ptr):
+        """Register (or, with dev_ptr 0 / None, unregister) a device buffer
+        that every step's last passes fill with derived field `kind`."""
+        _check(self.lib.fvm_set_display_field(self.h, int(kind), C.c_void_p(dev_ptr or None)))
 
     def save_checkpoint(self, path):
         """Write the solve (state, parameters, time-step state) to a checkpoint file."""

@@ -192,6 +192,17 @@ enum fvm_field_kind {
     FVM_FIELD_MACH = 4
 };
 int fvm_field_to_device(fvm_handle *h, int kind, float *dev_dst);
+/* Registers a display field (no reference counterpart; an extension for the
+ * application's per-frame compute*ToDevice call): from the next step on, the
+ * last passes of every step also write field `kind` of the new state into
+ * dev_dst (nx*ny floats, the layout of fvm_field_to_device), the same values
+ * a derived-field pass after the step writes.  fvm_field_to_device(kind,
+ * dev_dst) then returns without a launch while the state is the one a step
+ * left (writing fields, reset, obstacle updates, checkpoint loads and the
+ * autotuner make it launch again).  dev_dst must stay valid while it is
+ * registered; dev_dst == NULL unregisters, and so do fvm_initialize and
+ * fvm_resize.  Changing the registration re-captures the step graphs. */
+int fvm_set_display_field(fvm_handle *h, int kind, float *dev_dst);
 /* CFDSolver::convertCellTypesToDevice (src/solver.cu:3452-3459). */
 int fvm_cell_types_to_device(fvm_handle *h, float *dev_dst);
 /* CFDSolver::generateVectorArrows (src/solver.cu:3809-3845); *n_vertices_out

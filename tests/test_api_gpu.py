@@ -322,3 +322,52 @@ def test_bounded_wait_expires_with_a_status_and_the_solve_goes_on():
     twin.step(3)
     s.synchronize()
     assert np.array_equal(s.fields().view(np.uint32), twin.fields().view(np.uint32))
+
+
+@pytest.mark.parametrize("name", ["euler_m3_circle", "ns_karman_re200"])
+def test_display_field_from_the_step_equals_the_derived_pass(name):
+    """A registered display field (fvm_set_display_field) is written by the
+    step's last passes and the ghost pass: bitwise the derived-field pass of
+    the state after the step, for every kind, solid and ghost cells included,
+    through graph replay and eager launches; fvm_field_to_device into it then
+    launches nothing; writing fields makes it stale; unregistered, the steps
+    leave the buffer alone."""
+    torch = pytest.importorskip("torch")
+    s, p, e = _solver(name, 160, 80)
+    p.dt = s.compute_dt()
+    n = p.nx * p.ny
+    assert (s.cell_types() == abi.CELL_GHOST).any()
+    ref = torch.empty(n, dtype=torch.float32, device="cuda")
+
+    def same(disp, kind):
+        s.field_to_device(kind, ref.data_ptr())  # a separate derived-field pass
+        s.synchronize()
+        torch.cuda.synchronize()
+        return torch.equal(disp.view(torch.int32), ref.view(torch.int32))
+
+    for kind in range(5):
+        disp = torch.full((n,), float("nan"), dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()  # the fill is on torch's stream, the steps on the solver's
+        s.set_display_field(kind, disp.data_ptr())
+        for steps, eager in ((1, False), (3, False), (2, True)):
+            s.set_kernel_timing(eager)
+            s.step(steps)
+            s.synchronize()
+            n0 = s.launch_count()
+            s.field_to_device(kind, disp.data_ptr())  # fresh: no launch
+            assert s.launch_count() == n0
+            assert same(disp, kind), (kind, steps, eager)
+        s.set_kernel_timing(False)
+        # a new state: the registered field is stale and is recomputed
+        s.write_fields(s.fields() * np.float32(1.001))
+        n0 = s.launch_count()
+        s.field_to_device(kind, disp.data_ptr())
+        assert s.launch_count() == n0 + 1
+        assert same(disp, kind)
+        s.set_display_field(kind, 0)
+        disp.fill_(float("nan"))
+        torch.cuda.synchronize()
+        s.step(2)
+        s.synchronize()
+        torch.cuda.synchronize()
+        assert torch.isnan(disp).all()

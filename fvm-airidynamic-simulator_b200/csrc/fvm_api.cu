@@ -466,6 +466,7 @@ extern "C" int fvm_reset(fvm_handle *h, const fvm_sim_params *p) {
     h->g.dx = p->dx;
     h->g.dy = p->dy;
     k_zero_scalars<<<1, 1, 0, h->stream>>>(h->sc);
+    h->launches_at_sc_copy = -1;  // the host copy of the scalars is out of date
     CK(cudaGetLastError());
     launch_init(h->g, h->Un, freestream(h->prm), h->stream);
     CK(cudaGetLastError());
@@ -656,15 +657,20 @@ static unsigned long long graph_key(fvm_handle *h) {
     return k;
 }
 
-static int check_device_error(fvm_handle *h) {
-    CK(cudaMemcpyAsync(h->h_sc, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
+// Status of the error word in the host copy of the device scalars.
+static int device_error_status(fvm_handle *h) {
     if (h->h_sc->err & kErrTimeout)
         return set_err(FVM_ERR_TIMEOUT, "a bounded device wait expired (error word 0x%x)", h->h_sc->err);
     if (h->h_sc->err & kErrSmemAlign)
         return set_err(FVM_ERR_CUDA, "shared-memory staging area not 128-byte aligned; step skipped (error word 0x%x)",
                        h->h_sc->err);
     return FVM_OK;
+}
+
+static int check_device_error(fvm_handle *h) {
+    CK(cudaMemcpyAsync(h->h_sc, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return device_error_status(h);
 }
 
 static int finish_steps(fvm_handle *h, fvm_sim_params *p, int n) {
@@ -789,6 +795,10 @@ extern "C" int fvm_synchronize(fvm_handle *h) {
     CHECK_HANDLE(h);
     CK(cudaStreamSynchronize(h->stream));
     resolve_timing(h);
+    // only kernels set the error word: when none was launched since
+    // fvm_queue_dt copied the device scalars (the reference's per-frame
+    // queue / synchronize / read sequence), that copy, complete now, holds it
+    if (h->launches == h->launches_at_sc_copy) return device_error_status(h);
     return check_device_error(h);
 }
 
@@ -837,6 +847,7 @@ extern "C" int fvm_queue_dt(fvm_handle *h, const fvm_sim_params *p) {
         h->cfl_valid = true;
     }
     CK(cudaMemcpyAsync(h->h_sc, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->stream));
+    h->launches_at_sc_copy = h->launches;
     return FVM_OK;
 }
 
@@ -1201,6 +1212,7 @@ extern "C" int fvm_debug_stage1(fvm_handle *h, float dt, int with_ghost, float *
                                 float *E, float *rho_e) {
     CHECK_INIT(h);
     k_set_scalars<<<1, 1, 0, h->stream>>>(h->sc, dt, 0.0f, 0);
+    h->launches_at_sc_copy = -1;
     CK(cudaGetLastError());
     float *Un = h->buf[BUF_N], *Us = h->buf[BUF_S];
     StepArgs a1 = step_args(h, Us, 1, 0, 1.0f);
@@ -1234,6 +1246,7 @@ extern "C" int fvm_debug_wait_timeout(fvm_handle *h, long long limit_cycles) {
     unsigned zero = 0;
     CK(cudaMemcpyAsync(&h->sc->err, &zero, sizeof(unsigned), cudaMemcpyHostToDevice, h->stream));
     CK(cudaStreamSynchronize(h->stream));
+    h->launches_at_sc_copy = -1;
     return r;
 }
 

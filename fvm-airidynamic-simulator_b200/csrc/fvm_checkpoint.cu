@@ -166,6 +166,7 @@ extern "C" int fvm_load_checkpoint(fvm_handle *h, const char *path, fvm_sim_para
     h->h_sc->cfl[0] = hd.cfl_speed;
     h->h_sc->cfl[1] = hd.cfl_nu;
     e = cudaMemcpyAsync(h->sc, h->h_sc, sizeof(DevScalars), cudaMemcpyHostToDevice, h->stream);
+    h->launches_at_sc_copy = -1;
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return ckerr(FVM_ERR_CUDA, cudaGetErrorString(e));
     h->dt_ready = (hd.flags & kFlagDtReady) != 0;

@@ -70,6 +70,7 @@ struct fvm_handle {
     std::map<std::string, std::pair<long long, double>> ktimes;
     std::vector<std::string> knames;
     long long launches = 0;
+    long long launches_at_sc_copy = -1;  // launches when fvm_queue_dt copied the device scalars
     size_t bytes = 0;
 };
 

@@ -104,6 +104,8 @@ struct StepArgs {
     int cfl;               // 0: none, 1: wave speed, 2: wave speed + kinematic viscosity
     float dt_scale;        // stage dt = sc->dt * dt_scale (0.5 for the viscous half steps)
     const DisplayDesc *disp;  // last pass of a step: display field of the output (dense nx*ny), or null
+    int early_launch;         // let the next kernel (a ghost pass) launch before this grid drains
+    int pdl;                  // host: launch with programmatic stream serialization
 };
 
 struct GhostArgs {

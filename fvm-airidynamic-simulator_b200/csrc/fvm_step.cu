@@ -16,6 +16,8 @@
 // by clamping the shared-memory column.
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
+#include <utility>
 
 #include "fvm_kernels.cuh"
 #include "fvm_pairx.cuh"
@@ -445,20 +447,24 @@ __global__ void __launch_bounds__(NT, 768 / NT)
     static_assert(L::total <= 227 * 1024, "shared memory");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned char *smem = aligned_smem(smem_raw);
-    if (smem_misaligned(smem, a.sc)) return;
+    const bool misaligned = (smem_addr_opaque(smem) & 127u) != 0u;
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bar_off);
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0 && !misaligned) {
         prefetch_tensormap(&tm_in);
         if (STAGE == 2) prefetch_tensormap(&tm_blend);
         for (int k = 0; k < L::NBAR; k++) mbar_init(&bars[k], 1);
         fence_barrier_init();
     }
+    // the prologue above overlaps the previous step kernel's tail
+    pdl_wait();
+    if (smem_misaligned(smem, a.sc)) return;
     RingPos rp{0, 0};
     float lmax = 0.0f;
     unsigned nbad = 0;
-    if (!stage_tile<NT, K, STAGE, SCHEME, LIM, DISP>(&tm_in, &tm_blend, a, blockIdx.x * L::W,
-                                                     blockIdx.y * a.rows_per_cta, smem, rp, lmax, nbad))
-        return;
+    const bool ok = stage_tile<NT, K, STAGE, SCHEME, LIM, DISP>(&tm_in, &tm_blend, a, blockIdx.x * L::W,
+                                                                blockIdx.y * a.rows_per_cta, smem, rp, lmax, nbad);
+    if (a.early_launch) pdl_trigger();
+    if (!ok) return;
     if (a.cfl) block_publish<NT>(lmax, 0.0f, nbad, a.sc);
 }
 
@@ -779,18 +785,23 @@ __global__ void __launch_bounds__(NT, 640 / NT) k_viscous(const __grid_constant_
     using L = ViscLayout<NT, K>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned char *smem = aligned_smem(smem_raw);
-    if (smem_misaligned(smem, a.sc)) return;
+    const bool misaligned = (smem_addr_opaque(smem) & 127u) != 0u;
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bar_off);
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0 && !misaligned) {
         prefetch_tensormap(&tm_in);
         for (int k = 0; k < L::KP; k++) mbar_init(&bars[k], 1);
         fence_barrier_init();
     }
+    // the prologue above overlaps the previous step kernel's tail
+    pdl_wait();
+    if (smem_misaligned(smem, a.sc)) return;
     RingPos rp{0, 0};
     float ls = 0.0f, ln = 0.0f;
     unsigned nbad = 0;
-    if (!viscous_tile<NT, K, DISP>(&tm_in, a, blockIdx.x * L::W, blockIdx.y * a.rows_per_cta, smem, rp, ls, ln, nbad))
-        return;
+    const bool ok =
+        viscous_tile<NT, K, DISP>(&tm_in, a, blockIdx.x * L::W, blockIdx.y * a.rows_per_cta, smem, rp, ls, ln, nbad);
+    if (a.early_launch) pdl_trigger();
+    if (!ok) return;
     if (a.cfl) block_publish<NT>(ls, ln, nbad, a.sc);
 }
 
@@ -823,6 +834,8 @@ __device__ __forceinline__ StepArgs batch_args(const BatchInst &I, int out_role,
     a.cfl = cfl;
     a.dt_scale = dts;
     a.disp = nullptr;
+    a.early_launch = 0;
+    a.pdl = 0;
     return a;
 }
 
@@ -1018,6 +1031,10 @@ __device__ __forceinline__ void ghost_publish(const GhostArgs &a, float ls, floa
 __global__ void __launch_bounds__(128) k_ghost(const GhostArgs a) {
     float ls = 0.0f, ln = 0.0f;
     unsigned nbad = 0;
+    pdl_wait();
+    // the few CTAs of this pass are all resident: the next step kernel may
+    // launch now (it waits for this grid's completion before reading)
+    pdl_trigger();
     ghost_chunk(a, blockIdx.x * 128, 128, ls, ln, nbad);
     ghost_publish(a, ls, ln, nbad, gridDim.x);
 }
@@ -1171,6 +1188,30 @@ cudaError_t prepare_step_kernels(const StageTune &tn) {
     return cudaErrorInvalidValue;
 }
 
+// Step kernels launch with programmatic stream serialization: each may start
+// while its predecessor in the stream drains (see pdl_wait / pdl_trigger);
+// FVM_NO_PDL set in the environment launches them plainly.
+static bool pdl_enabled() {
+    static const bool on = getenv("FVM_NO_PDL") == nullptr;
+    return on;
+}
+
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_step_kernel(bool pdl, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                                      cudaStream_t st, Args &&...args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = (pdl && pdl_enabled()) ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
+
 template <int NT, int K, int STAGE, int SCHEME, int LIM>
 static cudaError_t launch_stage_t(const StageTune &tn, const CUtensorMap &tm_in, const CUtensorMap &tm_blend,
                                   const StepArgs &a, cudaStream_t st) {
@@ -1179,8 +1220,7 @@ static cudaError_t launch_stage_t(const StageTune &tn, const CUtensorMap &tm_in,
     auto kern = (STAGE == 2 && a.disp) ? k_stage<NT, K, STAGE, SCHEME, LIM, STAGE == 2>
                                        : k_stage<NT, K, STAGE, SCHEME, LIM, false>;
     dim3 grid((a.g.nx + L::W - 1) / L::W, (a.g.ny + a.rows_per_cta - 1) / a.rows_per_cta);
-    kern<<<grid, NT, L::total, st>>>(tm_in, tm_blend, a);
-    return cudaGetLastError();
+    return launch_step_kernel(a.pdl != 0, kern, grid, dim3(NT), L::total, st, tm_in, tm_blend, a);
 }
 
 template <int NT, int K, int STAGE>
@@ -1208,8 +1248,7 @@ static cudaError_t launch_viscous_t(const CUtensorMap &tm_in, const StepArgs &a,
     using L = ViscLayout<NT, K>;
     auto kern = a.disp ? k_viscous<NT, K, true> : k_viscous<NT, K, false>;
     dim3 grid((a.g.nx + L::W - 1) / L::W, (a.g.ny + a.rows_per_cta - 1) / a.rows_per_cta);
-    kern<<<grid, NT, L::total, st>>>(tm_in, a);
-    return cudaGetLastError();
+    return launch_step_kernel(a.pdl != 0, kern, grid, dim3(NT), L::total, st, tm_in, a);
 }
 
 cudaError_t launch_viscous(const StageTune &tn, const CUtensorMap &tm_in, const StepArgs &a, cudaStream_t st) {
@@ -1321,8 +1360,7 @@ cudaError_t launch_set_display(DisplayDesc *d, float *ptr, int kind, cudaStream_
 cudaError_t launch_ghost(const GhostArgs &a, cudaStream_t st) {
     int blocks = (a.n + 127) / 128;
     if (blocks < 1) blocks = 1;
-    k_ghost<<<blocks, 128, 0, st>>>(a);
-    return cudaGetLastError();
+    return launch_step_kernel(true, k_ghost, dim3(blocks), dim3(128), 0, st, a);
 }
 
 cudaError_t launch_bc_phase1(const GridDesc &g, float *U, const uint8_t *mask, const Freestream &fs, cudaStream_t st) {

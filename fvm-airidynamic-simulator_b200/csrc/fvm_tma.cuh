@@ -84,6 +84,16 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
         : "memory");
 }
 
+// Programmatic dependent launch: a step kernel launched with programmatic
+// stream serialization may start while its predecessor's last CTAs finish.
+// pdl_wait blocks until the predecessor grid has completed and its memory
+// operations are visible (a no-op without a programmatic dependency); code
+// before it must not read what the predecessor writes.  pdl_trigger lets
+// the successor launch once every CTA of this grid has issued it or exited;
+// the successor still waits for this grid's completion before reading.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" :::); }
+
 __device__ __forceinline__ void prefetch_tensormap(const CUtensorMap *map) {
     asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
 }

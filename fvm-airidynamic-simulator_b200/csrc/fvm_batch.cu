@@ -153,9 +153,13 @@ static int enqueue_batch_step(fvm_batch *b) {
         BCK(launch_viscous_batch(tn, b->d_insts, b->d_visc_tiles, b->n_visc_tiles, 0, st));
         b->launches++;
     }
-    BCK(launch_stage_batch(1, sch, lim, tn, b->d_insts, b->d_stage_tiles, b->n_stage_tiles, st));
+    // launches as in a single solve's step: stage 1 and an Euler-only stage 2
+    // let the ghost pass after them launch early; with viscous instances the
+    // post half step follows stage 2, which then launches plainly
+    const bool visc = b->n_visc_tiles > 0;
+    BCK(launch_stage_batch(1, sch, lim, tn, b->d_insts, b->d_stage_tiles, b->n_stage_tiles, 1, true, st));
     BCK(launch_ghost_batch(b->d_insts, b->d_chunks, b->n_chunks, 1, st));
-    BCK(launch_stage_batch(2, sch, lim, tn, b->d_insts, b->d_stage_tiles, b->n_stage_tiles, st));
+    BCK(launch_stage_batch(2, sch, lim, tn, b->d_insts, b->d_stage_tiles, b->n_stage_tiles, visc ? 0 : 1, !visc, st));
     b->launches += 3;
     if (b->n_visc_tiles) {
         BCK(launch_viscous_batch(tn, b->d_insts, b->d_visc_tiles, b->n_visc_tiles, 1, st));

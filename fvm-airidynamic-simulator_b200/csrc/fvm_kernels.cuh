@@ -35,8 +35,10 @@ cudaError_t launch_stage(int stage, int scheme, int limiter, const StageTune &tn
 // cells, copy elsewhere; optional phase-1 BC and CFL reduction.
 cudaError_t launch_viscous(const StageTune &tn, const CUtensorMap &tm_in, const StepArgs &a, cudaStream_t st);
 // Batched launches over a multi-instance tile list (persistent grids).
+// early: let the next kernel launch before this grid drains (a ghost pass
+// follows); pdl: launch with programmatic stream serialization
 cudaError_t launch_stage_batch(int stage, int scheme, int limiter, const StageTune &tn, const BatchInst *insts,
-                               const TileDesc *tiles, int ntiles, cudaStream_t st);
+                               const TileDesc *tiles, int ntiles, int early, bool pdl, cudaStream_t st);
 cudaError_t launch_viscous_batch(const StageTune &tn, const BatchInst *insts, const TileDesc *tiles, int ntiles,
                                  int post, cudaStream_t st);
 cudaError_t launch_ghost_batch(const BatchInst *insts, const GhostChunk *chunks, int nchunks, int mode,

@@ -841,7 +841,8 @@ __device__ __forceinline__ StepArgs batch_args(const BatchInst &I, int out_role,
 
 template <int NT, int K, int STAGE, int SCHEME, int LIM>
 __global__ void __launch_bounds__(NT, 640 / NT) k_stage_batch(const BatchInst *__restrict__ insts,
-                                                    const TileDesc *__restrict__ tiles, int ntiles, int rows) {
+                                                    const TileDesc *__restrict__ tiles, int ntiles, int rows,
+                                                    int early_launch) {
     using L = StageLayout<NT, K, STAGE>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ StepArgs s_args;
@@ -852,6 +853,9 @@ __global__ void __launch_bounds__(NT, 640 / NT) k_stage_batch(const BatchInst *_
         for (int k = 0; k < L::NBAR; k++) mbar_init(&bars[k], 1);
         fence_barrier_init();
     }
+    // the prologue above overlaps the previous kernel's tail; the buffer
+    // roles (device parity) and the states are read after the wait
+    pdl_wait();
     RingPos rp{0, 0};
     for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
         const TileDesc td = tiles[ti];
@@ -882,6 +886,7 @@ __global__ void __launch_bounds__(NT, 640 / NT) k_stage_batch(const BatchInst *_
             return;
         if (cfl) block_publish<NT>(lmax, 0.0f, nbad, I.sc);
     }
+    if (early_launch) pdl_trigger();
 }
 
 template <int NT, int K>
@@ -898,6 +903,7 @@ __global__ void __launch_bounds__(NT, 640 / NT) k_viscous_batch(const BatchInst 
         for (int k = 0; k < L::KP; k++) mbar_init(&bars[k], 1);
         fence_barrier_init();
     }
+    pdl_wait();
     RingPos rp{0, 0};
     for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
         const TileDesc td = tiles[ti];
@@ -913,6 +919,7 @@ __global__ void __launch_bounds__(NT, 640 / NT) k_viscous_batch(const BatchInst 
             return;
         if (post) block_publish<NT>(ls, ln, nbad, I.sc);
     }
+    if (post) pdl_trigger();  // a ghost pass follows the post half step
 }
 
 // ------------------------------------------------------------- ghost pass
@@ -1043,6 +1050,8 @@ __global__ void __launch_bounds__(128) k_ghost(const GhostArgs a) {
 // mode 1 = after stage 1, mode 2 = end of step (CFL, finalize, parity flip).
 __global__ void __launch_bounds__(128) k_ghost_batch(const BatchInst *__restrict__ insts,
                                                     const GhostChunk *__restrict__ chunks, int mode) {
+    pdl_wait();
+    pdl_trigger();
     const GhostChunk ch = chunks[blockIdx.x];
     const BatchInst &I = insts[ch.inst];
     const bool visc = I.viscous != 0;
@@ -1272,30 +1281,32 @@ static int persistent_grid(KERN kern, int threads, size_t smem, int ntiles) {
 
 template <int NT, int K, int STAGE, int SCHEME, int LIM>
 static cudaError_t launch_stage_batch_t(const BatchInst *insts, const TileDesc *tiles, int ntiles, int rows,
-                                        cudaStream_t st) {
+                                        int early, bool pdl, cudaStream_t st) {
     using L = StageLayout<NT, K, STAGE>;
     auto kern = k_stage_batch<NT, K, STAGE, SCHEME, LIM>;
     const int grid = persistent_grid(kern, NT, L::total, ntiles);
-    kern<<<grid, NT, L::total, st>>>(insts, tiles, ntiles, rows);
-    return cudaGetLastError();
+    return launch_step_kernel(pdl, kern, dim3(grid), dim3(NT), L::total, st, insts, tiles, ntiles, rows, early);
 }
 
 template <int NT, int K, int STAGE>
 static cudaError_t launch_stage_batch_s(int scheme, int lim, const BatchInst *insts, const TileDesc *tiles,
-                                        int ntiles, int rows, cudaStream_t st) {
-    if (scheme == 0 && lim == 0) return launch_stage_batch_t<NT, K, STAGE, 0, 0>(insts, tiles, ntiles, rows, st);
-    if (scheme == 0 && lim == 1) return launch_stage_batch_t<NT, K, STAGE, 0, 1>(insts, tiles, ntiles, rows, st);
-    if (scheme == 1 && lim == 0) return launch_stage_batch_t<NT, K, STAGE, 1, 0>(insts, tiles, ntiles, rows, st);
-    return launch_stage_batch_t<NT, K, STAGE, 1, 1>(insts, tiles, ntiles, rows, st);
+                                        int ntiles, int rows, int early, bool pdl, cudaStream_t st) {
+#define FVM_SBT(A, B) launch_stage_batch_t<NT, K, STAGE, A, B>(insts, tiles, ntiles, rows, early, pdl, st)
+    if (scheme == 0 && lim == 0) return FVM_SBT(0, 0);
+    if (scheme == 0 && lim == 1) return FVM_SBT(0, 1);
+    if (scheme == 1 && lim == 0) return FVM_SBT(1, 0);
+    return FVM_SBT(1, 1);
+#undef FVM_SBT
 }
 
 cudaError_t launch_stage_batch(int stage, int scheme, int limiter, const StageTune &tn, const BatchInst *insts,
-                               const TileDesc *tiles, int ntiles, cudaStream_t st) {
+                               const TileDesc *tiles, int ntiles, int early, bool pdl, cudaStream_t st) {
     if (ntiles <= 0) return cudaSuccess;
-#define FVM_SB(NT, K)                                                                                         \
-    if (tn.nt == NT && tn.ring == K)                                                                          \
-        return stage == 1 ? launch_stage_batch_s<NT, K, 1>(scheme, limiter, insts, tiles, ntiles, tn.rows, st) \
-                          : launch_stage_batch_s<NT, K, 2>(scheme, limiter, insts, tiles, ntiles, tn.rows, st);
+#define FVM_SB(NT, K)                                                                                             \
+    if (tn.nt == NT && tn.ring == K)                                                                              \
+        return stage == 1                                                                                         \
+                   ? launch_stage_batch_s<NT, K, 1>(scheme, limiter, insts, tiles, ntiles, tn.rows, early, pdl, st) \
+                   : launch_stage_batch_s<NT, K, 2>(scheme, limiter, insts, tiles, ntiles, tn.rows, early, pdl, st);
     FVM_SB(128, 4) FVM_SB(128, 6) FVM_SB(256, 4) FVM_SB(256, 6)
 #undef FVM_SB
     return cudaErrorInvalidValue;
@@ -1306,8 +1317,8 @@ static cudaError_t launch_viscous_batch_t(const BatchInst *insts, const TileDesc
                                           int post, cudaStream_t st) {
     auto kern = k_viscous_batch<NT, K>;
     const int grid = persistent_grid(kern, NT, ViscLayout<NT, K>::total, ntiles);
-    kern<<<grid, NT, ViscLayout<NT, K>::total, st>>>(insts, tiles, ntiles, rows, post);
-    return cudaGetLastError();
+    return launch_step_kernel(true, kern, dim3(grid), dim3(NT), ViscLayout<NT, K>::total, st, insts, tiles, ntiles,
+                              rows, post);
 }
 
 cudaError_t launch_viscous_batch(const StageTune &tn, const BatchInst *insts, const TileDesc *tiles, int ntiles,
@@ -1323,8 +1334,7 @@ cudaError_t launch_viscous_batch(const StageTune &tn, const BatchInst *insts, co
 cudaError_t launch_ghost_batch(const BatchInst *insts, const GhostChunk *chunks, int nchunks, int mode,
                                cudaStream_t st) {
     if (nchunks <= 0) return cudaSuccess;
-    k_ghost_batch<<<nchunks, 128, 0, st>>>(insts, chunks, mode);
-    return cudaGetLastError();
+    return launch_step_kernel(true, k_ghost_batch, dim3(nchunks), dim3(128), 0, st, insts, chunks, mode);
 }
 
 // Failure-path probe: one warp waits, through the kernels' own bounded wait,

@@ -239,18 +239,21 @@ struct TuneKey {
 static std::map<TuneKey, StageTune> g_tune_cache;
 
 // Default launch shape before (or without) autotuning: 128 threads, a 4-row
-// input ring, and the tallest tile in {64, 32, 16, 8, 4} rows that still gives
-// at least three CTAs per SM.  Small grids are latency-bound and want many
-// short tiles (measured on B200: 512x256 runs 1.6x faster at 4 rows than at
-// 16; 1024x512 is fastest at 8), large ones want tall tiles (64 at
-// 8192x4096), which keep the per-tile halo rows cheap.
-static StageTune heuristic_tune(int nx, int ny) {
+// input ring and about 48 row bands: the tile height in {4, 8, 16, ..., 64}
+// nearest ny / 48.  Measured on B200 (NS step): 1024x512 fastest at 8 rows
+// (0.071 ms; 10 and 12 rows 0.080 / 0.077), 2048x1024 at 24 (0.181 ms; 32 rows
+// 0.197), 4096x2048 at 40-48 (0.614 ms; 64 rows 0.661), 8192x4096 at 64;
+// 512x256 wants 4.  Small grids are latency-bound and want many short tiles,
+// large ones tall tiles, which keep the per-tile halo rows cheap.
+static StageTune heuristic_tune(int, int ny) {
     StageTune t{128, 4, 4};
-    const long long strips = (nx + t.nt - 5) / (t.nt - 4);
-    for (int rows : {64, 32, 16, 8}) {
-        if (strips * ((ny + rows - 1) / rows) >= 148LL * 3) {
+    const double want = ny / 48.0;
+    double best = 1e30;
+    for (int rows : {4, 8, 16, 24, 32, 40, 48, 56, 64}) {
+        const double d = rows > want ? rows - want : want - rows;
+        if (d < best) {
+            best = d;
             t.rows = rows;
-            break;
         }
     }
     return t;

@@ -207,6 +207,8 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
     const int j1 = min(j0 + a.rows_per_cta, ny);
     const int rs = j0 - 2;
     const int npairs = (j1 - j0 + 5) / 2;  // incoming rows rs .. j1+1 (one spare row when odd)
+    // steps 1 .. qx_end hold rows of the tile (rows r, r+1 meet [j0, j1))
+    const int qx_end = (j1 - j0 + 1) / 2;
     const float dt = a.sc->dt * a.dt_scale;
     const UpdateArgs ua{dt, 1.0f / g.dx, 1.0f / g.dy};
 
@@ -370,6 +372,10 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
 #pragma unroll
         for (int k = 0; k < 5; k++) fyB[k] = Fy[k].y;
         vfB = vfy.y;
+        // x-slopes and x-faces of rows r, r+1 feed only the update of those
+        // rows: none for the halo pairs above and below the tile (step 0 and,
+        // for an even tile height, the last step; uniform over the CTA)
+        const bool xrows = (unsigned)(q - 1) < (unsigned)qx_end;
         // x-slopes of rows r, r+1 at staged column t+1 (columns 1 .. NT-2 are
         // the cells beside the x-faces of phase 3)
         if (t < NT - 2) {
@@ -398,7 +404,7 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
             }
         }
         // ---- phase 3: x-faces of rows r, r+1 (read by the update in step q+1)
-        {
+        if (xrows) {
             f2 Fx[5];
             const float4 *A = PA + s0 * NT, *B = PB + s0 * NT;
             const uint32_t mb0 = M[pc0 * NT + tx + 1], mb1 = M[(pc0 + 1) * NT + tx + 1];

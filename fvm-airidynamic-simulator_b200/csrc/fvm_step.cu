@@ -291,6 +291,19 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
             ok_all = false;
             break;
         }
+        // step 0 stages only: its y-faces lie below the tile's first update,
+        // its rows take no x-faces, it issues no load, and nothing it would
+        // write is read before the next step's first barrier (the y-slopes of
+        // row r-2 it leaves at zero feed only the unused face (j0-2 | j0-1)).
+        // Stage 1 only: in stage 2 the extra path cost more than it saved.
+        if (STAGE == 1 && q == 0) {
+            pc1 = pc0;
+            pc0 = 2 - pc0;
+            kr = ring_next<KP>(kr);
+            par ^= (kr == 0) ? 1 : 0;
+            ku = ring_next<KP>(ku);
+            continue;
+        }
         // ---- phase 2: y-faces of column cy, then the update of rows r-2, r-1
         // column cy, rows r-3 .. r: pairs q-2 (rows r-4, r-3), q-1 (r-2, r-1), q (r, r+1)
         const float4 A1 = PA[s1 * NT + cy], B1 = PB[s1 * NT + cy];

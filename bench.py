@@ -58,7 +58,7 @@ STEP_BYTES_NS = 184
 # DRAM bytes (read + write) per launch measured by ncu on the 4096x2048 case
 # and scaled by the cell count to 8192x4096 (profiles/marching_kernels_*.md).
 MEASURED_TRAFFIC = {
-    ("ns_hypersonic_cone", 8192, 4096): {"stage1": 1261507584, "stage2": 1929546752,
+    ("ns_hypersonic_cone", 8192, 4096): {"stage1": 1250917376, "stage2": 1926714368,
                                          "viscous_pre": 1254623232, "viscous_post": 1235197952},
 }
 

@@ -4,6 +4,9 @@
 # (--use_fast_math -O3, CMakeLists.txt:277-298) retargeted to sm_100a:
 #   oracle/_ref/libfvm_ref.so      src/solver.cu + oracle/ref_harness.cu
 #   oracle/_ref/kernel_benchmark   src/solver.cu + src/test/kernel_benchmark.cu
+#   oracle/_ref/libcmap_ref.so     the colour-table generators and the field
+#                                  fragment shader of src/renderer.cpp, compiled
+#                                  for the host by oracle/ref_colormap.py
 # Test infrastructure only.  The reference checkout is $FVM_REFERENCE when
 # set, else a directory named `reference` beside this repository; when
 # neither holds the reference sources the script says so and does nothing
@@ -26,5 +29,9 @@ fi
 if [ ! -f "$OUT/kernel_benchmark" ]; then
     "$NVCC" $FLAGS -I"$REF/src/include" "$REF/src/test/kernel_benchmark.cu" "$REF/src/solver.cu" \
         -o "$OUT/kernel_benchmark"
+fi
+# the renderer's colour tables and field shader as a host library (libcmap_ref.so)
+if [ ! -f "$OUT/libcmap_ref.so" ] || [ "$HERE/ref_colormap.py" -nt "$OUT/libcmap_ref.so" ]; then
+    "${PYTHON:-python3}" "$HERE/ref_colormap.py" "$REF" "$OUT"
 fi
 echo "build_ref: built $OUT"

@@ -1,6 +1,11 @@
 """Colour images (fvm_colormap_*): the renderer's colour tables (CPU) and the
 field pass on the GPU against the oracle's CPU restatement of the fragment
-shader on the same derived field."""
+shader on the same derived field.  The restatement and the library's tables
+are pinned to the reference's own renderer code: tests/golden/ref_colormap.npz
+holds the outputs of its colour-table generators and of its field fragment
+shader compiled for the host (tests/golden/make_golden_colormap.py)."""
+import os
+
 import numpy as np
 import pytest
 
@@ -13,6 +18,34 @@ from oracle import oracle
 @pytest.mark.parametrize("cmap", range(5))
 def test_library_tables_equal_the_oracle_tables(cmap):
     assert np.array_equal(fvm_b200.colormap_table(cmap), oracle.colormap_table(cmap))
+
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_colormap.npz")
+
+
+@pytest.fixture(scope="module")
+def golden():
+    return np.load(GOLDEN)
+
+
+@pytest.mark.parametrize("cmap", range(5))
+def test_tables_equal_the_reference_generators(golden, cmap):
+    """Renderer::generate*Colormap (src/renderer.cpp:672-800): bit-exact."""
+    ref = golden["tables"][cmap]
+    assert np.array_equal(oracle.colormap_table(cmap), ref)
+    assert np.array_equal(fvm_b200.colormap_table(cmap), ref)
+
+
+@pytest.mark.parametrize("cmap", range(5))
+def test_oracle_shader_equals_the_reference_shader(golden, cmap):
+    """FIELD_FRAGMENT_SHADER (src/renderer.cpp:47-77) on every golden sample
+    (texel centres and edges, both clamped ends, a degenerate range, every
+    cell class 0..4): bit-exact in FP32."""
+    field, ct = golden["field"], golden["cell_type"]
+    assert set(np.unique(ct)) == {0, 1, 2, 3, 4}
+    for r, (lo, hi) in enumerate(golden["ranges"]):
+        got = oracle.colormap(field, ct, cmap, float(lo), float(hi), fmt=0)
+        assert np.array_equal(got, golden["rgba"][r, cmap]), (r, cmap)
 
 
 def test_table_end_points():

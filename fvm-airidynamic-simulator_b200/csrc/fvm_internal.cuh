@@ -55,26 +55,23 @@ struct DevScalars {
 // FVM_FIELD_*).  Used by the derived-field pass and, for a registered display
 // field, by the last passes of a step.
 __device__ __forceinline__ float derived_value(int kind, float rho, float rho_u, float rho_v, float rho_e) {
+    // the quotients by rho + 1e-10 share one approximate reciprocal (the one
+    // the fast-math division multiplies by)
+    const float irv = rcp_approx(rho + 1e-10f);
     switch (kind) {
-    case 0: {
-        float e = rho_e / (rho + 1e-10f);
-        return (GAMMA - 1.0f) * e / R_GAS;
-    }
+    case 0: return (GAMMA - 1.0f) * (rho_e * irv) * (1.0f / R_GAS);
     case 1: return (GAMMA - 1.0f) * rho_e;
     case 2: return rho;
     case 3: {
-        float rv = rho + 1e-10f;
-        float u = rho_u / rv, v = rho_v / rv;
+        const float u = rho_u * irv, v = rho_v * irv;
         return sqrtf(u * u + v * v);
     }
     default: {
-        float rv = rho + 1e-10f;
-        float u = rho_u / rv, v = rho_v / rv;
-        float speed = sqrtf(u * u + v * v);
-        float e = rho_e / rv;
-        float T = (GAMMA - 1.0f) * e / R_GAS;
-        float cs = sqrtf(GAMMA * R_GAS * T);
-        return speed / (cs + 1e-10f);
+        const float u = rho_u * irv, v = rho_v * irv;
+        const float speed = sqrtf(u * u + v * v);
+        const float T = (GAMMA - 1.0f) * (rho_e * irv) * (1.0f / R_GAS);
+        const float cs = sqrtf(GAMMA * R_GAS * T);
+        return speed * rcp_approx(cs + 1e-10f);
     }
     }
 }

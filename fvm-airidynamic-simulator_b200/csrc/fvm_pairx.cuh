@@ -38,10 +38,12 @@ __device__ __forceinline__ f2 p_min(f2 a, f2 b) { return mk2(fminf(a.x, b.x), fm
 __device__ __forceinline__ f2 p_max(f2 a, f2 b) { return mk2(fmaxf(a.x, b.x), fmaxf(a.y, b.y)); }
 __device__ __forceinline__ f2 p_max(f2 a, float b) { return mk2(fmaxf(a.x, b), fmaxf(a.y, b)); }
 __device__ __forceinline__ f2 p_sqrt(f2 a) { return mk2(sqrtf(a.x), sqrtf(a.y)); }
-// per-lane division a / b, the fast approximate form the scalar path uses
-__device__ __forceinline__ f2 p_div(f2 a, f2 b) { return mk2(__fdividef(a.x, b.x), __fdividef(a.y, b.y)); }
 // per-lane approximate reciprocal, shared by quotients with one divisor
 __device__ __forceinline__ f2 p_rcp(f2 a) { return mk2(rcp_approx(a.x), rcp_approx(a.y)); }
+// division a / b in the fast approximate form the scalar path uses
+// (__fdividef: a times the approximate reciprocal of b, flushed to zero for
+// |b| > 2^126), with the two products packed into one instruction
+__device__ __forceinline__ f2 p_div(f2 a, f2 b) { return p_mul(a, p_rcp(b)); }
 // per-lane approximate reciprocal square root
 __device__ __forceinline__ f2 p_rsqrt(f2 a) { return mk2(rsqrtf(a.x), rsqrtf(a.y)); }
 __device__ __forceinline__ f2 p_sel(bool cx, bool cy, f2 a, f2 b) { return mk2(cx ? a.x : b.x, cy ? a.y : b.y); }

@@ -385,9 +385,10 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tm_in, const CUten
 #pragma unroll
         for (int k = 0; k < 5; k++) fyB[k] = Fy[k].y;
         vfB = vfy.y;
-        // x-slopes and x-faces of rows r, r+1 feed only the update of those
-        // rows: none for the halo pairs above and below the tile (step 0 and,
-        // for an even tile height, the last step; uniform over the CTA)
+        // the x-faces of rows r, r+1 feed only the update of those rows: none
+        // for the halo pairs above and below the tile (step 0 and, for an even
+        // tile height, the last step; uniform over the CTA).  The x-slopes
+        // below stay unconditional: skipping them too made stage 2 spill.
         const bool xrows = (unsigned)(q - 1) < (unsigned)qx_end;
         // x-slopes of rows r, r+1 at staged column t+1 (columns 1 .. NT-2 are
         // the cells beside the x-faces of phase 3)

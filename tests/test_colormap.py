@@ -48,6 +48,26 @@ def test_oracle_shader_equals_the_reference_shader(golden, cmap):
         assert np.array_equal(got, golden["rgba"][r, cmap]), (r, cmap)
 
 
+def test_reference_extraction_on_a_synthetic_renderer():
+    """oracle/ref_colormap.py takes the generators as free functions and the
+    shader's main body with single-precision literals."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "ref_colormap", os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle",
+                                     "ref_colormap.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    gens = "".join(f"void Renderer::generate{n}Colormap(std::vector<float> &colors)\n{{\n    if (1) {{ colors[0] = 0.5f; }}\n}}\n"
+                   for n in mod.GENERATORS)
+    shader = ('const char *FIELD_FRAGMENT_SHADER = R"(\n#version 330 core\nuniform float minVal;\n'
+              'void main() {\n    float a = clamp(x / (y + 0.0001), 0.0, 1.0);\n    vec4 c = vec4(0.3, 0.3, 0.3, 1.0);\n}\n)";\n')
+    out_gens, body = mod.extract(gens + shader)
+    assert len(out_gens) == 5 and all(g.startswith("static void generate") for g in out_gens)
+    assert all("Renderer::" not in g and g.rstrip().endswith("}") for g in out_gens)
+    assert "0.0001f" in body and "clamp(x / (y + 0.0001f), 0.0f, 1.0f)" in body
+    assert "vec4(0.3f, 0.3f, 0.3f, 1.0f)" in body and "uniform" not in body
+
+
 def test_table_end_points():
     jet, hot = fvm_b200.colormap_table(abi.CMAP_JET), fvm_b200.colormap_table(abi.CMAP_HOT)
     assert tuple(jet[0]) == (0.0, 0.0, 0.5) and tuple(jet[255]) == (0.5, 0.0, 0.0)

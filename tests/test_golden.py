@@ -49,6 +49,28 @@ def test_oracle_fp64_reproduces_reference_steps(path):
     assert linf.max() <= 1e-3, dict(zip(FIELDS, linf))
 
 
+@pytest.mark.parametrize("mistake", ["ausm_plus_flux", "dt_plus_1pct"])
+@pytest.mark.parametrize("path", DYN, ids=[os.path.basename(f)[4:-4] for f in DYN])
+def test_a_planted_mistake_fails_the_golden_check(path, mistake):
+    """The check above is sensitive: the FP64 oracle with a mistake planted
+    in it (AUSM+ in place of the reference's HLLC, or every step 1 % too
+    long) misses the reference's state by more than the L1 tolerance."""
+    z = np.load(path)
+    p = _params(z)
+    e = abi.ext_default()
+    dt = float(z["dt"])
+    if mistake == "ausm_plus_flux":
+        e.flux_scheme = abi.FLUX_AUSM_PLUS
+    else:
+        dt *= 1.01
+    o = Oracle(p, e, bits=64)
+    o.set_geometry(z["sdf"], z["ct"])
+    o.set_fields(z["U0"])
+    for _ in range(int(z["steps"])):
+        o.step(dt)
+    assert rel_l1(z["U1"], o.fields()).max() > 1e-4
+
+
 @pytest.mark.parametrize("path", DYN, ids=[os.path.basename(f)[4:-4] for f in DYN])
 def test_oracle_reset_matches_reference_away_from_ghosts(path):
     """Freestream + boundary conditions: identical to the reference except at
